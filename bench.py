@@ -1,0 +1,378 @@
+#!/usr/bin/env python3
+"""
+Throughput of the kinematic-diffraction hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one 3-D intensity volume: one (snapshot, reflection) evaluation of all atoms,
+their four FFT components and the |S Amp|^2 + fftshift epilogue.  The workload is the
+two-phase polar-vortex film of 512 x 512 x 104 cells (5 atoms, 2 phases), alternating
+between the reflections G = (0,0,2) and (1,0,3) on one resident snapshot; the inputs are
+seeded synthetic fields (qpop_diffraction_b200.workloads.config2_*), since the reference
+ships no dataset at this size.
+
+Printed (rank 0, one JSON line):
+  value     Gcells/s over all ranks, inputs resident in HBM (packed float32 P, u, int8 phase)
+            and the intensity left in HBM; device time by CUDA events, max over ranks;
+  e2e       the same metric through the reference-facing C-ABI call qpd_run_host: float64
+            host arrays in pinned memory, host->device copies, packing, the transform and the
+            float64 intensity copied back, all inside the timed region;
+  roofline  the dominant kernel's algorithmic bytes per launch / its mean event-timed duration,
+            against the measured HBM copy bandwidth;
+  cpu_baseline  the oracle (a NumPy restatement of the reference's diffraction()) on a bounded
+            sample of the same workload, on this host's cores;
+  fp64      the same hand-written kernels in float64, fused and plain (the reference's own
+            per-atom, per-component schedule), for the float32-vs-float64 comparison.
+
+With --impl reference only the CPU oracle runs (rank 0), on bounded samples of the workload.
+Under torchrun each rank evaluates its own volumes on its own GPU (replicas: the path has no
+cross-volume exchange), so scaling is weak.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+GRID = (512, 512, 104)
+REFLECTIONS = ((0, 0, 2), (1, 0, 3))
+METRIC = "Gcells/s per 3-D volume at 512x512x104 (float32 source+FFT, float64 phase reduction)"
+UNIT = "Gcells/s"
+CPU_SAMPLE = (128, 128, 104)        # cpu_baseline: about 10 s of NumPy work
+REF_SAMPLE = (64, 64, 104)          # --impl reference: one step, so K + W steps end in minutes
+FALLBACK_HBM = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--grid", type=int, nargs=3, default=GRID)
+    ap.add_argument("--e2e-steps", type=int, default=None, help="steps of the host-buffer leg (default: min(K, 20))")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison leg")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id):
+        self.device_id = device_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device_id), "-lms", "50"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.reader.join(timeout=2)
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def atom_groups(R):
+    """Field counts of the fused schedule: g1 = distinct (R_x, R_y), g2 = distinct R_x."""
+    return len({(r[0], r[1]) for r in R}), len({r[0] for r in R})
+
+
+def kernel_bytes(n, g1, g2, weight):
+    """Algorithmic HBM bytes per launch of each fused kernel (float32 inputs, complex64 fields, float64 I)."""
+    b_in = 24 + 1 + (4 if weight else 0)
+    return {"zstage": n * (b_in + 3 * g1 * 8), "ypass": n * (3 * g1 * 8 + 2 * g2 * 8), "xpass": n * (2 * g2 * 8 + 8)}
+
+
+def profiled_traffic():
+    """DRAM bytes per cell of each fused kernel from the committed ncu summary (profiles/), if present."""
+    out = {}
+    for p in sorted((ROOT / "profiles").glob("*.md")):
+        for line in p.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_cell"):
+                for item in line.split()[1:]:
+                    k, _, v = item.partition("=")
+                    out[k] = float(v)
+    return out
+
+
+def cpu_oracle_rate(shape, threads):
+    """Cells/s of the oracle (the reference's NumPy diffraction(), restated) on the config-2 snapshot."""
+    from oracle import diffraction_oracle as oracle
+    from qpop_diffraction_b200 import workloads
+    case = workloads.config2(shape=shape, hkl=REFLECTIONS[0])
+    t = time.perf_counter()
+    oracle.diffraction(*case.args(), threads=threads)
+    dt = time.perf_counter() - t
+    return case.params.n / dt, dt
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from oracle import diffraction_oracle as oracle
+    from qpop_diffraction_b200 import workloads
+    threads = oracle.default_threads(5)
+    cases = [workloads.config2(shape=REF_SAMPLE, hkl=h) for h in REFLECTIONS]
+    for i in range(args.warmup):
+        oracle.diffraction(*cases[i % 2].args(), threads=threads)
+    t = time.perf_counter()
+    for i in range(args.steps):
+        oracle.diffraction(*cases[i % 2].args(), threads=threads)
+    dt = time.perf_counter() - t
+    n = cases[0].params.n
+    value = args.steps * n / dt / 1e9
+    sample = f"config-2 snapshot cropped to {'x'.join(map(str, REF_SAMPLE))}, both reflections alternating"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"two-phase vortex film {'x'.join(map(str, GRID))}, 5 atoms, G=002,103",
+                   "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    shape = tuple(args.grid)
+    params, oPhase, oStruc, u, region = workloads.config2_snapshot(seed=2 + rank, shape=shape)
+    n = params.n
+    spacing = (params.dx, params.dy, params.dz)
+    crystals = [crystal_from(params, workloads.config2_crystal(2, h)) for h in REFLECTIONS]
+    g1, g2 = atom_groups(crystals[0].R)
+
+    def plans_for(precision, schedule):
+        ps = []
+        for c in crystals:
+            p = Plan(shape, spacing, 2, 3, precision=precision, schedule=schedule, device=local)
+            p.set_crystal(c)
+            ps.append(p)
+        return ps
+
+    host = {k: torch.from_numpy(a) for k, a in (("oPhase", oPhase), ("oStruc", oStruc), ("u", u), ("region", region))}
+    d64 = {k: t.to(dev) for k, t in host.items()}
+
+    # ---------------- value: device-resident inputs ----------------
+    plans = plans_for("fp32", "fused")
+    packed = plans[0].pack(d64["oPhase"], d64["oStruc"], d64["u"], d64["region"])
+    out = torch.empty(shape, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(ps, inputs, i):
+        ps[i % 2].run_device(inputs, out)
+
+    for i in range(args.warmup):
+        step(plans, packed, i)
+    torch.cuda.synchronize(dev)
+    for p in plans:
+        p.stage_times()
+        p.enable_timing(True)
+    launches0 = sum(p.launches for p in plans)
+    smi_id = getattr(torch.cuda.get_device_properties(dev), "uuid", None)
+    smi_id = f"GPU-{smi_id}" if smi_id is not None else str(local)
+    with Clocks(smi_id) as clocks:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(plans, packed, i)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = sum(p.launches for p in plans) - launches0
+    stage = {}
+    for p in plans:
+        for k, (t, c) in p.stage_times().items():
+            s = stage.setdefault(k, [0.0, 0])
+            s[0] += t
+            s[1] += c
+        p.enable_timing(False)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps * n / (ms * 1e-3) / 1e9
+
+    hbm, hbm_src = peaks()
+    weight = packed["weight"] is not None
+    kb = kernel_bytes(n, g1, g2, weight)
+    per_kernel = {}
+    for k, (t, c) in stage.items():
+        avg = t / c
+        per_kernel[k] = {"launches": c, "avg_ms": avg, "bytes_per_launch": kb.get(k),
+                         "gbs": kb[k] / (avg * 1e-3) / 1e9 if k in kb else None}
+    dom = max(per_kernel, key=lambda k: stage[k][0])
+    traffic = profiled_traffic()
+    roof = {"bound": "hbm", "kernel": dom, "achieved": per_kernel[dom]["gbs"], "peak": hbm, "unit": "GB/s",
+            "frac": per_kernel[dom]["gbs"] / hbm, "peak_source": f"hbm_gbs of {hbm_src}",
+            "traffic": traffic[dom] * n if dom in traffic else None}
+    model_bytes = n * 5 * (25 + 144)
+    model = {"bytes_per_cell": 5 * (25 + 144), "achieved_gbs": model_bytes / (ms / args.steps * 1e-3) / 1e9,
+             "frac": model_bytes / (ms / args.steps * 1e-3) / 1e9 / hbm}
+
+    # ---------------- e2e: the C-ABI call with host buffers ----------------
+    ke = args.e2e_steps if args.e2e_steps is not None else min(args.steps, 20)
+    pinned = {k: t.pin_memory() for k, t in host.items()}
+    pin_np = {k: t.numpy() for k, t in pinned.items()}
+    I_host = torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+    plans[0].run_host(pin_np["oPhase"], pin_np["oStruc"], pin_np["u"], pin_np["region"], out=I_host)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for i in range(ke):
+        plans[i % 2].run_host(pin_np["oPhase"], pin_np["oStruc"], pin_np["u"], pin_np["region"], out=I_host)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = sum(a.nbytes for a in pin_np.values())
+    e2e = {"value": world * ke * n / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": I_host.nbytes, "steps": ke, "ms_per_step": e2e_s / ke * 1e3,
+           "call": "qpd_run_host (float64 host arrays, pinned)"}
+    for p in plans:
+        p.close()
+    del packed
+
+    # ---------------- float64: the same kernels, fused and plain ----------------
+    fp64 = None
+    if not args.no_fp64:
+        fp64 = {}
+        for schedule, k in (("fused", min(args.steps, 10)), ("plain", min(args.steps, 3))):
+            ps = plans_for("fp64", schedule)
+            pk = ps[0].pack(d64["oPhase"], d64["oStruc"], d64["u"], d64["region"])
+            for i in range(2):
+                step(ps, pk, i)
+            torch.cuda.synchronize(dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for i in range(k):
+                step(ps, pk, i)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            t = a.elapsed_time(b) / k
+            fp64[schedule] = {"value": n / (t * 1e-3) / 1e9, "ms_per_step": t, "steps": k}
+            for p in ps:
+                p.close()
+            del pk
+        for v in fp64.values():
+            v["fp32_speedup"] = v["ms_per_step"] / (ms / args.steps)
+
+    # ---------------- CPU baseline ----------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import diffraction_oracle as oracle
+        threads = oracle.default_threads(5)
+        rate, dt = cpu_oracle_rate(CPU_SAMPLE, threads)
+        cpu = {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"oracle (NumPy restatement of the reference diffraction()) on the config-2 snapshot cropped "
+                         f"to {'x'.join(map(str, CPU_SAMPLE))}, G=002, one run of {dt:.1f} s, "
+                         f"{threads} atom threads on {os.cpu_count()} host cores"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 snapshot)",
+            "config": {"workload": f"two-phase polar-vortex film {'x'.join(map(str, shape))}, 5 atoms, 2 phases, "
+                                   f"G=002,103 alternating", "grid": list(shape), "cells": n, "atoms": 5, "phases": 2,
+                       "precision": "fp32 fields, fp64 phase reduction, fp64 intensity", "schedule": "fused",
+                       "l2": "no flush: every step reads and writes about 4 GB, far above the 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roof, "model_roofline": model, "kernels": per_kernel, "gpu_launches": launches,
+            "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu, "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1024 @@
+// libqpopdiff.so: the C ABI declared in include/qpopdiff.h.
+//
+// Host side of the B200 diffraction path: axis planning (radix factorisation, twiddle tables),
+// crystal tables (atom grouping for the fused schedule, per-axis phase factors, voxel shape
+// factor), workspace management under an HBM budget, and the launch sequence of both schedules.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "qpopdiff.h"
+#include "qpd_kernels.cuh"
+
+using namespace qpd;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct qpd_ctx {
+    int device = 0;
+    uint64_t budget = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    size_t held = 0;
+
+    // plan
+    bool planned = false;
+    int64_t nx = 0, ny = 0, nz = 0, n = 0;
+    double h[3] = {0, 0, 0};
+    int nPhase = 0, nStruc = 0, precision = QPD_FP32, schedule = QPD_SCHED_FUSED;
+    std::vector<int> radix[3];
+    DevMem tw[3];
+
+    // crystal
+    bool have_crystal = false;
+    int nAtom = 0;
+    int sched_used = QPD_SCHED_FUSED;  // fused falls back to plain when the grouping does not fit
+    int ng1 = 0, ng2 = 0;
+    std::vector<int> grp;              // group of each atom in processing order
+    double tq[3] = {0, 0, 0};
+    double scale2 = 0;
+    DevMem tables;                     // complex coefficient tables, shape factors, constants, segments
+    // offsets into `tables`
+    size_t off_apc = 0, off_coefE = 0, off_coefUz = 0, off_S[3] = {0, 0, 0}, off_segY = 0, off_segX = 0;
+    size_t off_pex = 0, off_pey = 0, off_pez = 0, off_k[3] = {0, 0, 0};
+    int nsegY = 0;
+
+    // workspace
+    DevMem fields;  // fused: 3 * ng1 fields; plain: buf + amp
+    DevMem packed;  // host path: P, U, phase, weight
+    DevMem dense;   // host path, dense weights
+    DevMem stage;   // host path, float64 staging
+    DevMem Idev;    // host path, intensity
+    DevMem flags;
+
+    // per-kernel timing
+    bool timing = false;
+    struct Rec {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+};
+
+namespace {
+
+int fail(qpd_ctx* c, int code, const char* fmt, ...) {
+    char msg[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(msg, sizeof msg, fmt, ap);
+    va_end(ap);
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define QPD_CU(ctx, call)                                                                                     \
+    do {                                                                                                      \
+        cudaError_t e_ = (call);                                                                              \
+        if (e_ != cudaSuccess)                                                                                \
+            return fail((ctx), QPD_ERR_CUDA, "%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define QPD_TRY(expr)          \
+    do {                       \
+        int r_ = (expr);       \
+        if (r_ != QPD_OK) return r_; \
+    } while (0)
+
+int dev_free(qpd_ctx* c, DevMem& m) {
+    if (m.p) {
+        cudaError_t e = cudaFree(m.p);
+        c->held -= m.bytes;
+        m.p = nullptr;
+        m.bytes = 0;
+        if (e != cudaSuccess) return fail(c, QPD_ERR_CUDA, "cudaFree: %s", cudaGetErrorString(e));
+    }
+    return QPD_OK;
+}
+
+// Make m hold at least `bytes` (contents not kept when it grows).
+int dev_reserve(qpd_ctx* c, DevMem& m, size_t bytes, const char* what) {
+    if (m.p && m.bytes >= bytes) return QPD_OK;
+    QPD_TRY(dev_free(c, m));
+    if (bytes == 0) return QPD_OK;
+    if (c->budget && c->held + bytes > c->budget)
+        return fail(c, QPD_ERR_NOMEM, "%s needs %zu bytes; the context holds %zu of its %llu-byte budget", what, bytes,
+                    c->held, (unsigned long long)c->budget);
+    cudaError_t e = cudaMalloc(&m.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        m.p = nullptr;
+        return fail(c, QPD_ERR_NOMEM, "%s: cudaMalloc of %zu bytes failed: %s", what, bytes, cudaGetErrorString(e));
+    }
+    m.bytes = bytes;
+    c->held += bytes;
+    return QPD_OK;
+}
+
+cudaEvent_t take_event(qpd_ctx* c) {
+    if (!c->pool.empty()) {
+        cudaEvent_t e = c->pool.back();
+        c->pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+// Event before a timed launch (nullptr when timing is off).
+int tstart(qpd_ctx* c, cudaStream_t st, cudaEvent_t* a) {
+    *a = nullptr;
+    if (!c->timing) return QPD_OK;
+    *a = take_event(c);
+    if (!*a) return fail(c, QPD_ERR_CUDA, "cudaEventCreate failed");
+    QPD_CU(c, cudaEventRecord(*a, st));
+    return QPD_OK;
+}
+
+// Event after it; the pair is kept for qpd_stage_times.
+int tstop(qpd_ctx* c, int kind, cudaStream_t st, cudaEvent_t a) {
+    c->launches++;
+    QPD_CU(c, cudaGetLastError());
+    if (!a) return QPD_OK;
+    cudaEvent_t b = take_event(c);
+    if (!b) return fail(c, QPD_ERR_CUDA, "cudaEventCreate failed");
+    QPD_CU(c, cudaEventRecord(b, st));
+    c->recs.push_back({kind, a, b});
+    return QPD_OK;
+}
+
+// Radix stages of an axis: as many 8s as the power of two allows (a leftover 2 turns an 8 into
+// 4 * 4), then the odd primes in increasing order.
+std::vector<int> factorise(int64_t N) {
+    std::vector<int> r;
+    int64_t m = N;
+    int e2 = 0;
+    while (m % 2 == 0) {
+        m /= 2;
+        e2++;
+    }
+    int n8 = e2 / 3, rem = e2 % 3;
+    for (int i = 0; i < n8; i++) r.push_back(8);
+    if (rem == 2) r.push_back(4);
+    if (rem == 1) {
+        if (n8 > 0) {
+            r.pop_back();
+            r.push_back(4);
+            r.push_back(4);
+        } else {
+            r.push_back(2);
+        }
+    }
+    for (int64_t p = 3; p * p <= m; p += 2)
+        while (m % p == 0) {
+            r.push_back((int)p);
+            m /= p;
+        }
+    if (m > 1) r.push_back((int)m);
+    return r;
+}
+
+// 2 pi numpy.fft.fftfreq(N, h)[i], in numpy's operation order.
+double wavenumber(int64_t i, int64_t N, double h) {
+    const double val = 1.0 / ((double)N * h);
+    const int64_t m = i <= (N - 1) / 2 ? i : i - N;
+    return 2.0 * M_PI * ((double)m * val);
+}
+
+// numpy.sinc
+double sinc_np(double x) {
+    const double y = M_PI * (x == 0.0 ? 1.0e-20 : x);
+    return std::sin(y) / y;
+}
+
+// exp(-i theta) as numpy evaluates exp(-1j * x * R): (cos theta, -sin theta)
+double2 expmi(double theta) { return make_double2(std::cos(theta), -std::sin(theta)); }
+
+
+template <typename T> C_t<T> to_c(double2 v) { return cmake<C_t<T>>((T)v.x, (T)v.y); }
+
+AxisPlan axis_plan(const qpd_ctx* c, int d) {
+    AxisPlan ap;
+    std::memset(&ap, 0, sizeof ap);
+    ap.N = (int)(d == 0 ? c->nx : d == 1 ? c->ny : c->nz);
+    ap.nstages = (int)c->radix[d].size();
+    for (int s = 0; s < ap.nstages; s++) ap.radix[s] = c->radix[d][s];
+    ap.tw = c->tw[d].p;
+    return ap;
+}
+
+// ------------------------------------------------------------------------------------------
+// Launch configurations.  EPT * NT bounds the complex values a CTA tile holds.
+// ------------------------------------------------------------------------------------------
+
+size_t max_smem(qpd_ctx* c) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    return (size_t)v;
+}
+
+template <typename K> int set_smem(qpd_ctx* c, K kernel, size_t bytes) {
+    if (bytes > 48 * 1024)
+        QPD_CU(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return QPD_OK;
+}
+
+struct Cfg {
+    int nt, ept;
+};
+
+// z stage / fftz: a tile of M columns (4 fields each for the z stage)
+const Cfg kZCfg[] = {{256, 16}, {512, 16}, {1024, 8}, {1024, 16}};
+// strided axis passes: a tile of N x Cz
+const Cfg kACfg[] = {{256, 16}, {512, 16}, {1024, 8}, {1024, 16}};
+
+int odd_stride(int nz) { return nz % 2 ? nz : nz + 1; }
+
+template <typename T> struct Impl {
+    using C = C_t<T>;
+
+    // ---------------- tables ----------------
+    static int set_crystal(qpd_ctx* c, const qpd_crystal* k) {
+        const int A = k->nAtom, NP = k->nPhase, NS = k->nStruc;
+        const double* R = k->R;
+        // groups: g2 by R_x, g1 by (R_x, R_y), g1 numbered in g2 order
+        std::vector<double> rx;
+        std::vector<int> g2a(A), g1a(A);
+        for (int a = 0; a < A; a++) {
+            int f = -1;
+            for (size_t i = 0; i < rx.size(); i++)
+                if (rx[i] == R[3 * a]) f = (int)i;
+            if (f < 0) {
+                f = (int)rx.size();
+                rx.push_back(R[3 * a]);
+            }
+            g2a[a] = f;
+        }
+        const int G2 = (int)rx.size();
+        std::vector<double> ry;     // R_y of each g1
+        std::vector<int> g2of;      // g2 of each g1
+        for (int g2 = 0; g2 < G2; g2++) {
+            const size_t first = ry.size();
+            for (int a = 0; a < A; a++) {
+                if (g2a[a] != g2) continue;
+                int f = -1;
+                for (size_t i = first; i < ry.size(); i++)
+                    if (ry[i] == R[3 * a + 1]) f = (int)i;
+                if (f < 0) {
+                    f = (int)ry.size();
+                    ry.push_back(R[3 * a + 1]);
+                    g2of.push_back(g2);
+                }
+                g1a[a] = f;
+            }
+        }
+        const int G1 = (int)ry.size();
+        std::vector<int> order(A);
+        for (int a = 0; a < A; a++) order[a] = a;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return g1a[x] < g1a[y]; });
+
+        int sched = c->schedule;
+        if (sched == QPD_SCHED_FUSED) {
+            int maxin = 0;
+            for (int g2 = 0; g2 < G2; g2++) {
+                int cnt = 0;
+                for (int g1 = 0; g1 < G1; g1++) cnt += g2of[g1] == g2;
+                maxin = std::max(maxin, 3 * cnt);
+            }
+            if (A > kMaxAtoms || maxin > kMaxSegIn || 2 * G2 > kMaxSegIn || G2 > kMaxSegs) sched = QPD_SCHED_PLAIN;
+        }
+        c->sched_used = sched;
+        c->nAtom = A;
+        c->ng1 = G1;
+        c->ng2 = G2;
+        c->grp.assign(A, 0);
+        for (int i = 0; i < A; i++) c->grp[i] = g1a[order[i]];
+        for (int d = 0; d < 3; d++) c->tq[d] = k->qC[d] / (2.0 * M_PI);
+        const double nV = (double)c->n * k->V;
+        c->scale2 = 1.0 / (nV * nV);
+
+        const int64_t N[3] = {c->nx, c->ny, c->nz};
+        std::vector<double> kd[3], S[3];
+        for (int d = 0; d < 3; d++) {
+            kd[d].resize(N[d]);
+            S[d].resize(N[d]);
+            for (int64_t i = 0; i < N[d]; i++) {
+                kd[d][i] = wavenumber(i, N[d], c->h[d]);
+                S[d][i] = sinc_np(kd[d][i] * c->h[d] / (2.0 * M_PI));
+            }
+        }
+
+        // host images of every table, laid out in one device buffer
+        std::vector<unsigned char> host;
+        auto place = [&](size_t bytes) {
+            size_t off = (host.size() + 255) & ~size_t(255);
+            host.resize(off + bytes);
+            return off;
+        };
+        c->off_apc = place(sizeof(AtomPhase<T>) * NP * A);
+        {
+            AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(host.data() + c->off_apc);
+            for (int p = 0; p < NP; p++)
+                for (int i = 0; i < A; i++) {
+                    const int a = order[i];
+                    AtomPhase<T>& e = apc[p * A + i];
+                    std::memset(&e, 0, sizeof e);
+                    for (int s = 0; s < 3; s++) {
+                        double b = 0.0;
+                        for (int d = 0; d < 3; d++) {
+                            const double su = s < NS ? k->su[((d * NS + s) * NP + p) * A + a] : 0.0;
+                            e.su[d * 3 + s] = (T)su;
+                            b += k->qC[d] * su;
+                        }
+                        e.bq[s] = b / (2.0 * M_PI);
+                    }
+                    e.fr = (T)k->f_re[p * A + a];
+                    e.fi = (T)k->f_im[p * A + a];
+                }
+        }
+        for (int d = 0; d < 3; d++) {
+            c->off_S[d] = place(sizeof(double) * N[d]);
+            std::memcpy(host.data() + c->off_S[d], S[d].data(), sizeof(double) * N[d]);
+        }
+        std::vector<Segment<T>> segY, segX;
+        if (sched == QPD_SCHED_FUSED) {
+            c->off_coefE = place(sizeof(C) * A * N[2]);
+            c->off_coefUz = place(sizeof(C) * A * N[2]);
+            C* cE = reinterpret_cast<C*>(host.data() + c->off_coefE);
+            C* cU = reinterpret_cast<C*>(host.data() + c->off_coefUz);
+            for (int i = 0; i < A; i++) {
+                const int a = order[i];
+                for (int64_t z = 0; z < N[2]; z++) {
+                    const double2 e = expmi((kd[2][z] + k->G[2]) * R[3 * a + 2]);
+                    cE[i * N[2] + z] = to_c<T>(e);
+                    cU[i * N[2] + z] = to_c<T>(make_double2(kd[2][z] * e.y, -kd[2][z] * e.x));  // -i k_z e
+                }
+            }
+            // y tables per g1: ey, -i k_y ey; x tables per g2: ex, -i k_x ex
+            std::vector<size_t> offY(G1), offX(G2);
+            for (int g1 = 0; g1 < G1; g1++) {
+                offY[g1] = place(sizeof(C) * 2 * N[1]);
+                C* t = reinterpret_cast<C*>(host.data() + offY[g1]);
+                for (int64_t y = 0; y < N[1]; y++) {
+                    const double2 e = expmi((kd[1][y] + k->G[1]) * ry[g1]);
+                    t[y] = to_c<T>(e);
+                    t[N[1] + y] = to_c<T>(make_double2(kd[1][y] * e.y, -kd[1][y] * e.x));
+                }
+            }
+            for (int g2 = 0; g2 < G2; g2++) {
+                offX[g2] = place(sizeof(C) * 2 * N[0]);
+                C* t = reinterpret_cast<C*>(host.data() + offX[g2]);
+                for (int64_t x = 0; x < N[0]; x++) {
+                    const double2 e = expmi((kd[0][x] + k->G[0]) * rx[g2]);
+                    t[x] = to_c<T>(e);
+                    t[N[0] + x] = to_c<T>(make_double2(kd[0][x] * e.y, -kd[0][x] * e.x));
+                }
+            }
+            // segments hold device addresses: filled in once the buffer exists
+            for (int g2 = 0; g2 < G2; g2++) {
+                Segment<T> s;
+                std::memset(&s, 0, sizeof s);
+                s.nout = 2;
+                s.out[0] = 2 * g2;
+                s.out[1] = 2 * g2 + 1;
+                for (int g1 = 0; g1 < G1; g1++) {
+                    if (g2of[g1] != g2) continue;
+                    for (int comp = 0; comp < 3; comp++) {
+                        s.in[s.nin] = 3 * g1 + comp;
+                        // store table offsets + 1 for now (0 = no contribution)
+                        const size_t e = offY[g1] + 1, mi = offY[g1] + sizeof(C) * N[1] + 1;
+                        if (comp == 0) s.coef[0][s.nin] = reinterpret_cast<const C*>(e);
+                        if (comp == 2) s.coef[0][s.nin] = reinterpret_cast<const C*>(mi);
+                        if (comp == 1) s.coef[1][s.nin] = reinterpret_cast<const C*>(e);
+                        s.nin++;
+                    }
+                }
+                segY.push_back(s);
+            }
+            Segment<T> s;
+            std::memset(&s, 0, sizeof s);
+            s.nout = 1;
+            for (int g2 = 0; g2 < G2; g2++) {
+                s.in[s.nin] = 2 * g2;
+                s.coef[0][s.nin++] = reinterpret_cast<const C*>(offX[g2] + 1);
+                s.in[s.nin] = 2 * g2 + 1;
+                s.coef[0][s.nin++] = reinterpret_cast<const C*>(offX[g2] + sizeof(C) * N[0] + 1);
+            }
+            segX.push_back(s);
+            c->nsegY = G2;
+            c->off_segY = place(sizeof(Segment<T>) * segY.size());
+            c->off_segX = place(sizeof(Segment<T>));
+        } else {
+            // plain: per-atom axis factors in double and the wavenumbers
+            c->off_pex = place(sizeof(double2) * A * N[0]);
+            c->off_pey = place(sizeof(double2) * A * N[1]);
+            c->off_pez = place(sizeof(double2) * A * N[2]);
+            const size_t offs[3] = {c->off_pex, c->off_pey, c->off_pez};
+            for (int d = 0; d < 3; d++) {
+                double2* t = reinterpret_cast<double2*>(host.data() + offs[d]);
+                for (int i = 0; i < A; i++) {
+                    const int a = order[i];
+                    for (int64_t m = 0; m < N[d]; m++) t[i * N[d] + m] = expmi((kd[d][m] + k->G[d]) * R[3 * a + d]);
+                }
+                c->off_k[d] = place(sizeof(double) * N[d]);
+                std::memcpy(host.data() + c->off_k[d], kd[d].data(), sizeof(double) * N[d]);
+            }
+            Segment<T> s;
+            std::memset(&s, 0, sizeof s);
+            s.nin = 1;
+            s.nout = 1;
+            s.ident = 1;
+            segX.push_back(s);
+            c->off_segX = place(sizeof(Segment<T>));
+        }
+        QPD_TRY(dev_reserve(c, c->tables, host.size(), "crystal tables"));
+        const uintptr_t base = reinterpret_cast<uintptr_t>(c->tables.p);
+        auto fix = [&](Segment<T>& s) {
+            for (int o = 0; o < 2; o++)
+                for (int i = 0; i < kMaxSegIn; i++)
+                    if (s.coef[o][i]) s.coef[o][i] = reinterpret_cast<const C*>(base + reinterpret_cast<uintptr_t>(s.coef[o][i]) - 1);
+        };
+        for (auto& s : segY) fix(s);
+        for (auto& s : segX) fix(s);
+        if (!segY.empty()) std::memcpy(host.data() + c->off_segY, segY.data(), sizeof(Segment<T>) * segY.size());
+        std::memcpy(host.data() + c->off_segX, segX.data(), sizeof(Segment<T>));
+        QPD_CU(c, cudaMemcpyAsync(c->tables.p, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
+        QPD_CU(c, cudaStreamSynchronize(c->stream));
+
+        const size_t fb = sched == QPD_SCHED_FUSED ? (size_t)3 * G1 * c->n * sizeof(C) : (size_t)2 * c->n * sizeof(C);
+        QPD_TRY(dev_reserve(c, c->fields, fb, "field workspace"));
+        return QPD_OK;
+    }
+
+    template <typename A> static A* tab(qpd_ctx* c, size_t off) {
+        return reinterpret_cast<A*>(static_cast<unsigned char*>(c->tables.p) + off);
+    }
+
+    // ---------------- launches ----------------
+    template <int NT, int EPT> static int launch_z(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
+        const int cap = NT * EPT / 4;
+        a.M = std::max(1, (int)std::min<int64_t>(cap / a.nz, a.ncols));
+        a.ps = odd_stride(a.nz);
+        const size_t smem = sizeof(C) * 4 * a.M * a.ps + sizeof(AtomPhase<T>) * a.in.nPhase * a.nAtom + 16;
+        QPD_TRY(set_smem(c, zstage_kernel<T, NT, EPT>, smem));
+        const int64_t grid = (a.ncols + a.M - 1) / a.M;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        zstage_kernel<T, NT, EPT><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_ZSTAGE, st, t0);
+    }
+
+    static int run_z(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
+        const size_t lim = max_smem(c);
+        for (const Cfg& f : kZCfg) {
+            const int cap = f.nt * f.ept / 4;
+            if (a.nz > cap) continue;
+            const int M = std::max(1, (int)std::min<int64_t>(cap / a.nz, a.ncols));
+            const size_t smem = sizeof(C) * 4 * M * odd_stride(a.nz) + sizeof(AtomPhase<T>) * a.in.nPhase * a.nAtom + 16;
+            if (smem > lim) continue;
+            if (f.nt == 256 && f.ept == 16) return launch_z<256, 16>(c, a, st);
+            if (f.nt == 512 && f.ept == 16) return launch_z<512, 16>(c, a, st);
+            if (f.nt == 1024 && f.ept == 8) return launch_z<1024, 8>(c, a, st);
+            if (f.nt == 1024 && f.ept == 16) return launch_z<1024, 16>(c, a, st);
+        }
+        return fail(c, QPD_ERR_UNSUPPORTED, "nz = %d is too long for the z stage in this precision", a.nz);
+    }
+
+    template <int NT, int EPT> static int launch_fftz(qpd_ctx* c, FftzArgs<T>& a, cudaStream_t st) {
+        a.M = std::max(1, (int)std::min<int64_t>(NT * EPT / a.nz, a.ncols));
+        a.ps = odd_stride(a.nz);
+        const size_t smem = sizeof(C) * a.M * a.ps + 16;
+        QPD_TRY(set_smem(c, fftz_kernel<T, NT, EPT>, smem));
+        const int64_t grid = (a.ncols + a.M - 1) / a.M;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        fftz_kernel<T, NT, EPT><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_FFTZ, st, t0);
+    }
+
+    static int run_fftz(qpd_ctx* c, FftzArgs<T>& a, cudaStream_t st) {
+        const size_t lim = max_smem(c);
+        for (const Cfg& f : kZCfg) {
+            const int cap = f.nt * f.ept;
+            if (a.nz > cap) continue;
+            const int M = std::max(1, (int)std::min<int64_t>(cap / a.nz, a.ncols));
+            if (sizeof(C) * M * odd_stride(a.nz) + 16 > lim) continue;
+            if (f.nt == 256 && f.ept == 16) return launch_fftz<256, 16>(c, a, st);
+            if (f.nt == 512 && f.ept == 16) return launch_fftz<512, 16>(c, a, st);
+            if (f.nt == 1024 && f.ept == 8) return launch_fftz<1024, 8>(c, a, st);
+            if (f.nt == 1024 && f.ept == 16) return launch_fftz<1024, 16>(c, a, st);
+        }
+        return fail(c, QPD_ERR_UNSUPPORTED, "nz = %d is too long for the z transform in this precision", a.nz);
+    }
+
+    template <int NT, int EPT, bool EPI>
+    static int launch_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        a.Cz = std::max(1, std::min(a.nz, NT * EPT / a.N));
+        a.nzc = (a.nz + a.Cz - 1) / a.Cz;
+        const size_t smem = sizeof(C) * a.N * a.Cz + 16;
+        QPD_TRY(set_smem(c, axis_kernel<T, NT, EPT, EPI>, smem));
+        const int64_t grid = nouter * a.nzc;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        axis_kernel<T, NT, EPT, EPI><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, kind, st, t0);
+    }
+
+    template <bool EPI> static int run_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        const size_t lim = max_smem(c);
+        int best = -1, bestCz = 0;
+        for (int i = 0; i < 4; i++) {
+            const Cfg& f = kACfg[i];
+            const int cap = f.nt * f.ept;
+            if (a.N > cap) continue;
+            const int Cz = std::min(a.nz, cap / a.N);
+            if (sizeof(C) * a.N * Cz + 16 > lim) continue;
+            // prefer a z chunk of up to 8 (64-byte rows in float32), then fewer threads
+            if (best < 0 || std::min(Cz, 8) > std::min(bestCz, 8)) {
+                best = i;
+                bestCz = Cz;
+            }
+        }
+        switch (best) {
+            case 0: return launch_axis<256, 16, EPI>(c, a, nouter, kind, st);
+            case 1: return launch_axis<512, 16, EPI>(c, a, nouter, kind, st);
+            case 2: return launch_axis<1024, 8, EPI>(c, a, nouter, kind, st);
+            case 3: return launch_axis<1024, 16, EPI>(c, a, nouter, kind, st);
+        }
+        return fail(c, QPD_ERR_UNSUPPORTED, "an axis of length %d is too long in this precision", a.N);
+    }
+
+    static Inputs<T> inputs(qpd_ctx* c, const void* P, const void* U, const int8_t* phase, const void* weight,
+                            const void* wdense) {
+        Inputs<T> in;
+        in.P = static_cast<const T*>(P);
+        in.U = static_cast<const T*>(U);
+        in.phase = reinterpret_cast<const signed char*>(phase);
+        in.weight = static_cast<const T*>(weight);
+        in.wdense = static_cast<const T*>(wdense);
+        in.n = c->n;
+        in.nStruc = c->nStruc;
+        in.nPhase = c->nPhase;
+        return in;
+    }
+
+    static int run_device(qpd_ctx* c, const Inputs<T>& in, double* I, cudaStream_t st) {
+        C* F = static_cast<C*>(c->fields.p);
+        const int64_t n = c->n;
+        if (c->sched_used == QPD_SCHED_FUSED) {
+            ZArgs<T> z;
+            std::memset(&z, 0, sizeof z);
+            z.in = in;
+            z.ncols = c->nx * c->ny;
+            z.nz = (int)c->nz;
+            z.nAtom = c->nAtom;
+            z.apc = tab<AtomPhase<T>>(c, c->off_apc);
+            z.coefE = tab<C>(c, c->off_coefE);
+            z.coefUz = tab<C>(c, c->off_coefUz);
+            for (int i = 0; i < c->nAtom; i++) z.grp[i] = c->grp[i];
+            z.out = F;
+            z.fstride = n;
+            for (int d = 0; d < 3; d++) z.tq[d] = c->tq[d];
+            z.zp = axis_plan(c, 2);
+            QPD_TRY(run_z(c, z, st));
+
+            AxisArgs<T> y;
+            std::memset(&y, 0, sizeof y);
+            y.N = (int)c->ny;
+            y.stride = c->nz;
+            y.ostride = c->ny * c->nz;
+            y.nz = (int)c->nz;
+            y.in = F;
+            y.out = F;
+            y.fstride = n;
+            y.segs = tab<Segment<T>>(c, c->off_segY);
+            y.nseg = c->nsegY;
+            y.ap = axis_plan(c, 1);
+            QPD_TRY(run_axis<false>(c, y, c->nx, QPD_K_YPASS, st));
+
+            AxisArgs<T> x;
+            std::memset(&x, 0, sizeof x);
+            x.N = (int)c->nx;
+            x.stride = c->ny * c->nz;
+            x.ostride = c->nz;
+            x.nz = (int)c->nz;
+            x.in = F;
+            x.fstride = n;
+            x.segs = tab<Segment<T>>(c, c->off_segX);
+            x.nseg = 1;
+            x.ap = axis_plan(c, 0);
+            x.I = I;
+            for (int d = 0; d < 3; d++) x.S[d] = tab<double>(c, c->off_S[d]);
+            x.scale2 = c->scale2;
+            x.nx = c->nx;
+            x.ny = c->ny;
+            return run_axis<true>(c, x, c->ny, QPD_K_XPASS, st);
+        }
+        // plain schedule
+        C* buf = F;
+        C* amp = F + n;
+        QPD_CU(c, cudaMemsetAsync(amp, 0, sizeof(C) * n, st));
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        for (int at = 0; at < c->nAtom; at++) {
+            for (int comp = 0; comp < 4; comp++) {
+                SourceArgs<T> s;
+                std::memset(&s, 0, sizeof s);
+                s.in = in;
+                s.apc = tab<AtomPhase<T>>(c, c->off_apc);
+                s.nAtom = c->nAtom;
+                s.at = at;
+                s.comp = comp;
+                for (int d = 0; d < 3; d++) s.tq[d] = c->tq[d];
+                s.buf = buf;
+                cudaEvent_t t0;
+                QPD_TRY(tstart(c, st, &t0));
+                source_kernel<T><<<blocks, 256, 0, st>>>(s);
+                QPD_TRY(tstop(c, QPD_K_SOURCE, st, t0));
+
+                FftzArgs<T> fz;
+                std::memset(&fz, 0, sizeof fz);
+                fz.buf = buf;
+                fz.ncols = c->nx * c->ny;
+                fz.nz = (int)c->nz;
+                fz.zp = axis_plan(c, 2);
+                QPD_TRY(run_fftz(c, fz, st));
+
+                for (int d = 1; d >= 0; d--) {
+                    AxisArgs<T> ax;
+                    std::memset(&ax, 0, sizeof ax);
+                    ax.N = (int)(d == 1 ? c->ny : c->nx);
+                    ax.stride = d == 1 ? c->nz : c->ny * c->nz;
+                    ax.ostride = d == 1 ? c->ny * c->nz : c->nz;
+                    ax.nz = (int)c->nz;
+                    ax.in = buf;
+                    ax.out = buf;
+                    ax.fstride = n;
+                    ax.segs = tab<Segment<T>>(c, c->off_segX);
+                    ax.nseg = 1;
+                    ax.ap = axis_plan(c, d);
+                    QPD_TRY(run_axis<false>(c, ax, d == 1 ? c->nx : c->ny, QPD_K_AXIS, st));
+                }
+
+                AccArgs<T> ac;
+                ac.amp = amp;
+                ac.buf = buf;
+                ac.ex = tab<double2>(c, c->off_pex) + (int64_t)at * c->nx;
+                ac.ey = tab<double2>(c, c->off_pey) + (int64_t)at * c->ny;
+                ac.ez = tab<double2>(c, c->off_pez) + (int64_t)at * c->nz;
+                ac.kd = comp > 0 ? tab<double>(c, c->off_k[comp - 1]) : nullptr;
+                ac.comp = comp;
+                ac.nx = c->nx;
+                ac.ny = c->ny;
+                ac.nz = c->nz;
+                cudaEvent_t t1;
+                QPD_TRY(tstart(c, st, &t1));
+                accumulate_kernel<T><<<blocks, 256, 0, st>>>(ac);
+                QPD_TRY(tstop(c, QPD_K_ACC, st, t1));
+            }
+        }
+        IntensityArgs<T> ia;
+        ia.I = I;
+        ia.amp = amp;
+        for (int d = 0; d < 3; d++) ia.S[d] = tab<double>(c, c->off_S[d]);
+        // the plain amplitude carries the 1/V of the per-atom factors only through scale2
+        ia.scale2 = c->scale2;
+        ia.nx = c->nx;
+        ia.ny = c->ny;
+        ia.nz = c->nz;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        intensity_kernel<T><<<blocks, 256, 0, st>>>(ia);
+        return tstop(c, QPD_K_INTENSITY, st, t0);
+    }
+
+    // float64 planes -> packed inputs, cells [g0, g0 + cnt); planes point at cell g0
+    static int pack(qpd_ctx* c, int64_t g0, int64_t cnt, const double* const* ost, const double* const* uu,
+                    const double* const* oph, const double* region, void* P, void* U, int8_t* phase, void* weight,
+                    void* wdense, uint32_t* flags, cudaStream_t st) {
+        PackArgs<T> a;
+        std::memset(&a, 0, sizeof a);
+        a.cnt = cnt;
+        a.g0 = g0;
+        a.n = c->n;
+        a.nStruc = c->nStruc;
+        a.nPhase = c->nPhase;
+        for (int k = 0; k < c->nStruc; k++) a.ost[k] = ost[k];
+        for (int k = 0; k < 3; k++) a.uu[k] = uu[k];
+        for (int p = 0; p < c->nPhase; p++) a.oph[p] = oph[p];
+        a.region = region;
+        a.P = static_cast<T*>(P);
+        a.U = static_cast<T*>(U);
+        a.phase = reinterpret_cast<signed char*>(phase);
+        a.weight = static_cast<T*>(weight);
+        a.wdense = static_cast<T*>(wdense);
+        a.flags = flags;
+        if (cnt <= 0) return QPD_OK;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        pack_kernel<T><<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(a);
+        return tstop(c, QPD_K_PACK, st, t0);
+    }
+
+    static int run_host(qpd_ctx* c, const double* oPhase, const double* oStruc, const double* u, const double* region,
+                        double* I) {
+        const int64_t n = c->n;
+        const int NS = c->nStruc, NP = c->nPhase;
+        const int planes = NS + 3 + NP + (region ? 1 : 0);
+        // packed inputs + intensity
+        const size_t pk = sizeof(T) * 6 * n + n + sizeof(T) * n;
+        QPD_TRY(dev_reserve(c, c->packed, pk, "packed inputs"));
+        QPD_TRY(dev_reserve(c, c->Idev, sizeof(double) * n, "intensity"));
+        QPD_TRY(dev_reserve(c, c->flags, 256, "flags"));
+        // staging of float64 planes, in chunks of whole cells
+        const int64_t chunk = std::min<int64_t>(n, (int64_t)1 << 23);
+        QPD_TRY(dev_reserve(c, c->stage, sizeof(double) * planes * chunk, "float64 staging"));
+        unsigned char* pb = static_cast<unsigned char*>(c->packed.p);
+        T* P = reinterpret_cast<T*>(pb);
+        T* U = P + 3 * n;
+        T* W = U + 3 * n;
+        int8_t* ph = reinterpret_cast<int8_t*>(W + n);
+        uint32_t* flags = static_cast<uint32_t*>(c->flags.p);
+        double* sg = static_cast<double*>(c->stage.p);
+        cudaStream_t st = c->stream;
+
+        auto stage_pass = [&](bool dense, void* wd) -> int {
+            for (int64_t g0 = 0; g0 < n; g0 += chunk) {
+                const int64_t cnt = std::min(chunk, n - g0);
+                const double* ost[3] = {nullptr, nullptr, nullptr};
+                const double* uu[3];
+                const double* oph[kMaxPhases];
+                int pl = 0;
+                auto put = [&](const double* src) -> const double* {
+                    double* dst = sg + (size_t)pl * chunk;
+                    pl++;
+                    cudaError_t e = cudaMemcpyAsync(dst, src + g0, sizeof(double) * cnt, cudaMemcpyHostToDevice, st);
+                    return e == cudaSuccess ? dst : nullptr;
+                };
+                for (int k = 0; k < NS; k++)
+                    if (!(ost[k] = put(oStruc + (int64_t)k * n))) return fail(c, QPD_ERR_CUDA, "host-to-device copy of oStruc failed");
+                for (int k = 0; k < 3; k++)
+                    if (!(uu[k] = put(u + (int64_t)k * n))) return fail(c, QPD_ERR_CUDA, "host-to-device copy of u failed");
+                for (int p = 0; p < NP; p++)
+                    if (!(oph[p] = put(oPhase + (int64_t)p * n))) return fail(c, QPD_ERR_CUDA, "host-to-device copy of oPhase failed");
+                const double* rg = nullptr;
+                if (region && !(rg = put(region))) return fail(c, QPD_ERR_CUDA, "host-to-device copy of region failed");
+                QPD_TRY(pack(c, g0, cnt, ost, uu, oph, rg, P, U, ph, W, dense ? wd : nullptr, flags, st));
+                // the staging buffer is reused by the next chunk's copies
+                QPD_CU(c, cudaStreamSynchronize(st));
+            }
+            return QPD_OK;
+        };
+
+        QPD_CU(c, cudaMemsetAsync(flags, 0, sizeof(uint32_t), st));
+        QPD_TRY(stage_pass(false, nullptr));
+        uint32_t f = 0;
+        QPD_CU(c, cudaMemcpyAsync(&f, flags, sizeof f, cudaMemcpyDeviceToHost, st));
+        QPD_CU(c, cudaStreamSynchronize(st));
+        Inputs<T> in;
+        if (f & 1u) {
+            QPD_TRY(dev_reserve(c, c->dense, sizeof(T) * NP * n, "dense phase weights"));
+            QPD_TRY(stage_pass(true, c->dense.p));
+            in = inputs(c, P, U, nullptr, nullptr, c->dense.p);
+        } else {
+            in = inputs(c, P, U, ph, (f & 2u) ? W : nullptr, nullptr);
+        }
+        double* Id = static_cast<double*>(c->Idev.p);
+        QPD_TRY(run_device(c, in, Id, st));
+        QPD_CU(c, cudaMemcpyAsync(I, Id, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        QPD_CU(c, cudaStreamSynchronize(st));
+        return QPD_OK;
+    }
+};
+
+int upload_twiddles(qpd_ctx* c, int d, int64_t N) {
+    std::vector<double2> w(N);
+    for (int64_t m = 0; m < N; m++) {
+        const double a = 2.0 * M_PI * (double)m / (double)N;
+        w[m] = make_double2(std::cos(a), -std::sin(a));
+    }
+    if (c->precision == QPD_FP64) {
+        QPD_TRY(dev_reserve(c, c->tw[d], sizeof(double2) * N, "twiddles"));
+        QPD_CU(c, cudaMemcpy(c->tw[d].p, w.data(), sizeof(double2) * N, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float2> f(N);
+        for (int64_t m = 0; m < N; m++) f[m] = make_float2((float)w[m].x, (float)w[m].y);
+        QPD_TRY(dev_reserve(c, c->tw[d], sizeof(float2) * N, "twiddles"));
+        QPD_CU(c, cudaMemcpy(c->tw[d].p, f.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+    }
+    return QPD_OK;
+}
+
+int use_device(qpd_ctx* c) {
+    QPD_CU(c, cudaSetDevice(c->device));
+    return QPD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
+    if (!out) return fail(nullptr, QPD_ERR_ARG, "qpd_create: out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) return fail(nullptr, QPD_ERR_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    if (device < 0 || device >= count) return fail(nullptr, QPD_ERR_ARG, "device %d outside 0..%d", device, count - 1);
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, QPD_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    qpd_ctx* c = new qpd_ctx();
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(nullptr, QPD_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return QPD_OK;
+}
+
+int qpd_destroy(qpd_ctx* c) {
+    if (!c) return QPD_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (DevMem* m : {&c->tw[0], &c->tw[1], &c->tw[2], &c->tables, &c->fields, &c->packed, &c->dense, &c->stage,
+                      &c->Idev, &c->flags})
+        dev_free(c, *m);
+    for (auto& r : c->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return QPD_OK;
+}
+
+const char* qpd_last_error(const qpd_ctx* c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int qpd_axis_radices(int64_t N, int32_t* radices, int32_t cap) {
+    if (N < 1) return QPD_ERR_ARG;
+    std::vector<int> r = factorise(N);
+    if (!radices || cap < (int)r.size()) return (int)r.size();
+    for (size_t i = 0; i < r.size(); i++) radices[i] = r[i];
+    return (int)r.size();
+}
+
+int qpd_plan(qpd_ctx* c, const qpd_grid* g, int32_t nPhase, int32_t nStruc, int32_t precision, int32_t schedule) {
+    if (!c || !g) return fail(c, QPD_ERR_ARG, "qpd_plan: NULL argument");
+    if (g->nx < 1 || g->ny < 1 || g->nz < 1) return fail(c, QPD_ERR_ARG, "grid %lld x %lld x %lld is empty",
+                                                         (long long)g->nx, (long long)g->ny, (long long)g->nz);
+    if (!(g->dx > 0 && g->dy > 0 && g->dz > 0)) return fail(c, QPD_ERR_ARG, "grid spacings must be positive");
+    if (nPhase < 1 || nPhase > kMaxPhases) return fail(c, QPD_ERR_ARG, "nPhase = %d outside 1..%d", nPhase, kMaxPhases);
+    if (nStruc < 0 || nStruc > 3) return fail(c, QPD_ERR_ARG, "nStruc = %d outside 0..3", nStruc);
+    if (precision != QPD_FP32 && precision != QPD_FP64) return fail(c, QPD_ERR_ARG, "unknown precision %d", precision);
+    if (schedule != QPD_SCHED_FUSED && schedule != QPD_SCHED_PLAIN) return fail(c, QPD_ERR_ARG, "unknown schedule %d", schedule);
+    if (g->nx > 16384 || g->ny > 16384 || g->nz > 4096)
+        return fail(c, QPD_ERR_UNSUPPORTED, "axis lengths above 16384 (x, y) or 4096 (z) are not supported");
+    const int64_t n = g->nx * g->ny * g->nz;
+    if (n > ((int64_t)1 << 40)) return fail(c, QPD_ERR_UNSUPPORTED, "grid of %lld cells is too large", (long long)n);
+    QPD_TRY(use_device(c));
+    c->planned = false;
+    c->have_crystal = false;
+    c->nx = g->nx;
+    c->ny = g->ny;
+    c->nz = g->nz;
+    c->n = n;
+    c->h[0] = g->dx;
+    c->h[1] = g->dy;
+    c->h[2] = g->dz;
+    c->nPhase = nPhase;
+    c->nStruc = nStruc;
+    c->precision = precision;
+    c->schedule = schedule;
+    const int64_t N[3] = {g->nx, g->ny, g->nz};
+    for (int d = 0; d < 3; d++) {
+        c->radix[d] = N[d] > 1 ? factorise(N[d]) : std::vector<int>();
+        if ((int)c->radix[d].size() > kMaxStages) return fail(c, QPD_ERR_UNSUPPORTED, "axis %d has too many stages", d);
+        QPD_TRY(upload_twiddles(c, d, N[d]));
+    }
+    c->planned = true;
+    return QPD_OK;
+}
+
+int qpd_set_crystal(qpd_ctx* c, const qpd_crystal* k) {
+    if (!c || !k) return fail(c, QPD_ERR_ARG, "qpd_set_crystal: NULL argument");
+    if (!c->planned) return fail(c, QPD_ERR_STATE, "qpd_set_crystal before qpd_plan");
+    if (k->nAtom < 1) return fail(c, QPD_ERR_ARG, "nAtom = %d", k->nAtom);
+    if (k->nPhase != c->nPhase || k->nStruc != c->nStruc)
+        return fail(c, QPD_ERR_ARG, "crystal has nPhase %d, nStruc %d; the plan %d, %d", k->nPhase, k->nStruc, c->nPhase,
+                    c->nStruc);
+    if (!k->R || !k->f_re || !k->f_im || (k->nStruc > 0 && !k->su)) return fail(c, QPD_ERR_ARG, "crystal arrays are NULL");
+    if (!(k->V != 0.0 && std::isfinite(k->V))) return fail(c, QPD_ERR_ARG, "cell volume V = %g", k->V);
+    QPD_TRY(use_device(c));
+    c->have_crystal = false;
+    int r = c->precision == QPD_FP64 ? Impl<double>::set_crystal(c, k) : Impl<float>::set_crystal(c, k);
+    if (r == QPD_OK) c->have_crystal = true;
+    return r;
+}
+
+int qpd_run_host(qpd_ctx* c, const double* oPhase, const double* oStruc, const double* u, const double* region,
+                 double* I) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_run_host: ctx is NULL");
+    if (!c->planned || !c->have_crystal) return fail(c, QPD_ERR_STATE, "qpd_run_host needs qpd_plan and qpd_set_crystal");
+    if (!oPhase || !u || !I || (c->nStruc > 0 && !oStruc)) return fail(c, QPD_ERR_ARG, "qpd_run_host: NULL array");
+    QPD_TRY(use_device(c));
+    return c->precision == QPD_FP64 ? Impl<double>::run_host(c, oPhase, oStruc, u, region, I)
+                                    : Impl<float>::run_host(c, oPhase, oStruc, u, region, I);
+}
+
+int qpd_pack_device(qpd_ctx* c, const double* oPhase, const double* oStruc, const double* u, const double* region,
+                    void* P, void* U, int8_t* phase, void* weight, void* wdense, int32_t dense, uint32_t* flags,
+                    void* stream) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_pack_device: ctx is NULL");
+    if (!c->planned) return fail(c, QPD_ERR_STATE, "qpd_pack_device before qpd_plan");
+    if (!oPhase || !u || !P || !U || (c->nStruc > 0 && !oStruc)) return fail(c, QPD_ERR_ARG, "qpd_pack_device: NULL array");
+    if (dense ? !wdense : (!phase || !weight)) return fail(c, QPD_ERR_ARG, "qpd_pack_device: NULL weight output");
+    QPD_TRY(use_device(c));
+    QPD_TRY(dev_reserve(c, c->flags, 256, "flags"));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    const int64_t n = c->n;
+    const double* ost[3] = {nullptr, nullptr, nullptr};
+    const double* uu[3];
+    const double* oph[kMaxPhases];
+    for (int k = 0; k < c->nStruc; k++) ost[k] = oStruc + k * n;
+    for (int k = 0; k < 3; k++) uu[k] = u + k * n;
+    for (int p = 0; p < c->nPhase; p++) oph[p] = oPhase + p * n;
+    uint32_t* fd = static_cast<uint32_t*>(c->flags.p);
+    QPD_CU(c, cudaMemsetAsync(fd, 0, sizeof(uint32_t), st));
+    int r = c->precision == QPD_FP64
+                ? Impl<double>::pack(c, 0, n, ost, uu, oph, region, P, U, phase, weight, dense ? wdense : nullptr, fd, st)
+                : Impl<float>::pack(c, 0, n, ost, uu, oph, region, P, U, phase, weight, dense ? wdense : nullptr, fd, st);
+    QPD_TRY(r);
+    uint32_t f = 0;
+    QPD_CU(c, cudaMemcpyAsync(&f, fd, sizeof f, cudaMemcpyDeviceToHost, st));
+    QPD_CU(c, cudaStreamSynchronize(st));
+    if (flags) *flags = f;
+    return QPD_OK;
+}
+
+int qpd_run_device(qpd_ctx* c, const void* P, const void* U, const int8_t* phase, const void* weight,
+                   const void* wdense, double* I_dev, void* stream) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_run_device: ctx is NULL");
+    if (!c->planned || !c->have_crystal) return fail(c, QPD_ERR_STATE, "qpd_run_device needs qpd_plan and qpd_set_crystal");
+    if (!P || !U || !I_dev || (!wdense && !phase)) return fail(c, QPD_ERR_ARG, "qpd_run_device: NULL array");
+    QPD_TRY(use_device(c));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    if (c->precision == QPD_FP64) {
+        Inputs<double> in = Impl<double>::inputs(c, P, U, phase, weight, wdense);
+        return Impl<double>::run_device(c, in, I_dev, st);
+    }
+    Inputs<float> in = Impl<float>::inputs(c, P, U, phase, weight, wdense);
+    return Impl<float>::run_device(c, in, I_dev, st);
+}
+
+int qpd_enable_timing(qpd_ctx* c, int32_t on) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_enable_timing: ctx is NULL");
+    c->timing = on != 0;
+    return QPD_OK;
+}
+
+int qpd_stage_times(qpd_ctx* c, double* ms, uint64_t* counts, int32_t cap) {
+    if (!c || !ms || !counts || cap < QPD_K_COUNT) return fail(c, QPD_ERR_ARG, "qpd_stage_times: bad arguments");
+    QPD_TRY(use_device(c));
+    for (int k = 0; k < QPD_K_COUNT; k++) {
+        ms[k] = 0.0;
+        counts[k] = 0;
+    }
+    int rc = QPD_OK;
+    for (auto& r : c->recs) {
+        float t = 0.0f;
+        cudaError_t e = cudaEventSynchronize(r.b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, r.a, r.b);
+        if (e != cudaSuccess && rc == QPD_OK) rc = fail(c, QPD_ERR_CUDA, "event timing: %s", cudaGetErrorString(e));
+        ms[r.kind] += t;
+        counts[r.kind]++;
+        c->pool.push_back(r.a);
+        c->pool.push_back(r.b);
+    }
+    c->recs.clear();
+    return rc;
+}
+
+uint64_t qpd_workspace_bytes(const qpd_ctx* c) { return c ? c->held : 0; }
+uint64_t qpd_launch_count(const qpd_ctx* c) { return c ? c->launches : 0; }
+
+}  // extern "C"

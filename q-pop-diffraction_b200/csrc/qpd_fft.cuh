@@ -1,0 +1,252 @@
+// Mixed-radix Stockham FFT over pencils held in shared memory.
+//
+// A CTA holds a tile of `count` pencils of length N in shared memory and transforms all of
+// them together, forward (exp(-2 pi i j k / N)), unnormalised, results in natural order.
+// Each radix-R stage reads a thread's butterflies into registers, applies the stage twiddles
+// and the R-point DFT, waits at a CTA barrier, and writes the results back in place in
+// Stockham (self-sorting) order: out[(j / Ns) Ns R + j % Ns + s Ns] = DFT_R(...)[s].
+// Butterflies are numbered pencil-fastest, so neighbouring threads touch neighbouring
+// pencils; tiles are laid out so that this is bank-conflict free (pencils contiguous,
+// or pencil strides odd in 8-byte words).
+#pragma once
+
+#include "qpd_common.cuh"
+
+namespace qpd {
+
+constexpr int kMaxStages = 24;
+
+// One axis of the transform, passed to kernels by value.  tw points to N complex values
+// exp(-2 pi i m / N), m = 0..N-1, computed in double on the host and stored in the kernel
+// precision.  radix[] multiplies out to N; an axis of length 1 has no stage.
+struct AxisPlan {
+    int N;
+    int nstages;
+    int radix[kMaxStages];
+    const void* tw;
+};
+
+// Where the pencils of a tile sit in shared memory: pencil pc starts at
+// (pc / group) * gstride + (pc % group) * pstride and its elements are estride apart.
+struct Pencils {
+    int count;
+    int group;
+    int gstride;
+    int pstride;
+    int estride;
+    __device__ __forceinline__ int base(int pc) const { return (pc / group) * gstride + (pc % group) * pstride; }
+};
+
+template <int R, typename C> struct Dft {
+    // Odd R: pair r with R - r, y[s] = x0 + sum_r (cos a_r - i sin b_r), y[R - s] = x0 + sum_r (cos a_r + i sin b_r),
+    // with a_r = x_r + x_{R-r}, b_r = x_r - x_{R-r}, angles 2 pi r s / R; w[m] = exp(-2 pi i m / R).
+    __device__ __forceinline__ static void run(C (&x)[R], const C (&w)[R]) {
+        static_assert(R % 2 == 1, "generic radix must be odd");
+        constexpr int H = (R - 1) / 2;
+        C a[H], b[H];
+#pragma unroll
+        for (int r = 1; r <= H; r++) {
+            a[r - 1] = cadd(x[r], x[R - r]);
+            b[r - 1] = csub(x[r], x[R - r]);
+        }
+        C y0 = x[0];
+#pragma unroll
+        for (int r = 0; r < H; r++) y0 = cadd(y0, a[r]);
+#pragma unroll
+        for (int s = 1; s <= H; s++) {
+            C A = x[0];
+            C B = cmake<C>(0, 0);
+#pragma unroll
+            for (int r = 1; r <= H; r++) {
+                const int m = (r * s) % R;
+                const auto c = w[m].x;
+                const auto sn = -w[m].y;
+                A.x = fma(c, a[r - 1].x, A.x);
+                A.y = fma(c, a[r - 1].y, A.y);
+                B.x = fma(sn, b[r - 1].x, B.x);
+                B.y = fma(sn, b[r - 1].y, B.y);
+            }
+            x[s] = cadd(A, cmul_mi(B));
+            x[R - s] = cadd(A, cmul_pi(B));
+        }
+        x[0] = y0;
+    }
+};
+
+template <typename C> struct Dft<2, C> {
+    __device__ __forceinline__ static void run(C (&x)[2], const C (&)[2]) {
+        C a = x[0];
+        x[0] = cadd(a, x[1]);
+        x[1] = csub(a, x[1]);
+    }
+};
+
+template <typename C> struct Dft<3, C> {
+    __device__ __forceinline__ static void run(C (&x)[3], const C (&)[3]) {
+        using R_t = decltype(C::x);
+        const R_t h = R_t(0.86602540378443864676);  // sqrt(3) / 2
+        C t = cadd(x[1], x[2]);
+        C m = cmake<C>(x[0].x - R_t(0.5) * t.x, x[0].y - R_t(0.5) * t.y);
+        C d = cscale(csub(x[1], x[2]), h);
+        x[0] = cadd(x[0], t);
+        x[1] = cadd(m, cmul_mi(d));
+        x[2] = cadd(m, cmul_pi(d));
+    }
+};
+
+template <typename C> __device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
+    C a = cadd(x0, x2), b = csub(x0, x2), c = cadd(x1, x3), d = cmul_mi(csub(x1, x3));
+    x0 = cadd(a, c);
+    x2 = csub(a, c);
+    x1 = cadd(b, d);
+    x3 = csub(b, d);
+}
+
+template <typename C> struct Dft<4, C> {
+    __device__ __forceinline__ static void run(C (&x)[4], const C (&)[4]) { dft4(x[0], x[1], x[2], x[3]); }
+};
+
+template <typename C> struct Dft<8, C> {
+    __device__ __forceinline__ static void run(C (&x)[8], const C (&)[8]) {
+        using R_t = decltype(C::x);
+        const R_t r2 = R_t(0.70710678118654752440);  // 1 / sqrt(2)
+        C e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
+        C o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
+        dft4(e0, e1, e2, e3);
+        dft4(o0, o1, o2, o3);
+        C t1 = cmake<C>((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);   // exp(-i pi / 4) o1
+        C t2 = cmul_mi(o2);                                         // exp(-i pi / 2) o2
+        C t3 = cmake<C>((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);  // exp(-3 i pi / 4) o3
+        x[0] = cadd(e0, o0);
+        x[4] = csub(e0, o0);
+        x[1] = cadd(e1, t1);
+        x[5] = csub(e1, t1);
+        x[2] = cadd(e2, t2);
+        x[6] = csub(e2, t2);
+        x[3] = cadd(e3, t3);
+        x[7] = csub(e3, t3);
+    }
+};
+
+template <int R> __host__ __device__ constexpr bool generic_radix() { return R != 2 && R != 3 && R != 4 && R != 8; }
+
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// One radix-R stage over all pencils of the tile, in place.  BPT bounds the butterflies
+// per thread: count * N <= EPT * nthreads with BPT = ceil(EPT / R).
+template <typename T, int R, int BPT>
+__device__ __forceinline__ void stage_r(C_t<T>* buf, const Pencils& pg, int N, int Ns, const C_t<T>* __restrict__ tw,
+                                        int tid, int nt) {
+    using C = C_t<T>;
+    const int L = N / R;
+    const int nb = pg.count * L;
+    const int tstep = N / (Ns * R);
+    C w[R];
+    if constexpr (generic_radix<R>()) {
+#pragma unroll
+        for (int m = 0; m < R; m++) w[m] = tw[m * L];
+    }
+    C v[BPT][R];
+    int ob[BPT];
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const int b = tid + q * nt;
+        if (b < nb) {
+            const int pc = b % pg.count;
+            const int j = b / pg.count;
+            const int k = j % Ns;
+            const int pb = pg.base(pc);
+#pragma unroll
+            for (int r = 0; r < R; r++) v[q][r] = buf[pb + (j + r * L) * pg.estride];
+            if (Ns > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], tw[r * k * tstep]);
+            }
+            Dft<R, C>::run(v[q], w);
+            ob[q] = pb + ((j / Ns) * Ns * R + k) * pg.estride;
+        }
+    }
+    __syncthreads();
+    const int os = Ns * pg.estride;
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const int b = tid + q * nt;
+        if (b < nb) {
+#pragma unroll
+            for (int r = 0; r < R; r++) buf[ob[q] + r * os] = v[q][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Any radix, one thread per output: y_s = sum_r x_r W_N^(r k N/(Ns R) + (r s mod R) N/R).
+// Used for prime factors without a specialised butterfly.
+template <typename T, int EPT>
+__device__ __noinline__ void stage_direct(C_t<T>* buf, const Pencils& pg, int N, int Ns, int R,
+                                          const C_t<T>* __restrict__ tw, int tid, int nt) {
+    using C = C_t<T>;
+    const int L = N / R;
+    const int ne = pg.count * N;
+    const int tstep = N / (Ns * R);
+    C out[EPT];
+    int oa[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT; q++) {
+        const int e = tid + q * nt;
+        if (e < ne) {
+            const int pc = e % pg.count;
+            const int rest = e / pg.count;
+            const int j = rest % L;
+            const int s = rest / L;
+            const int k = j % Ns;
+            const int pb = pg.base(pc);
+            C acc = cmake<C>(0, 0);
+            for (int r = 0; r < R; r++) {
+                int idx = r * k * tstep + ((r * s) % R) * L;
+                if (idx >= N) idx -= N;
+                cfma(acc, buf[pb + (j + r * L) * pg.estride], tw[idx]);
+            }
+            out[q] = acc;
+            oa[q] = pb + ((j / Ns) * Ns * R + k + s * Ns) * pg.estride;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < EPT; q++) {
+        const int e = tid + q * nt;
+        if (e < ne) buf[oa[q]] = out[q];
+    }
+    __syncthreads();
+}
+
+// Radices with a register butterfly; any other factor goes through stage_direct.
+__host__ __device__ constexpr bool fast_radix(int r) {
+    return r == 2 || r == 3 || r == 4 || r == 5 || r == 7 || r == 8 || r == 11 || r == 13 || r == 17;
+}
+
+// Forward FFT of every pencil of the tile.  All threads of the CTA must call it.
+template <typename T, int EPT>
+__device__ void fft_pencils(C_t<T>* buf, const Pencils& pg, const AxisPlan& ap, int tid, int nt) {
+    using C = C_t<T>;
+    const C* tw = static_cast<const C*>(ap.tw);
+    const int N = ap.N;
+    int Ns = 1;
+    for (int s = 0; s < ap.nstages; s++) {
+        const int R = ap.radix[s];
+        switch (R) {
+            case 2: stage_r<T, 2, cdiv(EPT, 2)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 3: stage_r<T, 3, cdiv(EPT, 3)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 4: stage_r<T, 4, cdiv(EPT, 4)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 5: stage_r<T, 5, cdiv(EPT, 5)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 7: stage_r<T, 7, cdiv(EPT, 7)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 8: stage_r<T, 8, cdiv(EPT, 8)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 11: stage_r<T, 11, cdiv(EPT, 11)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 13: stage_r<T, 13, cdiv(EPT, 13)>(buf, pg, N, Ns, tw, tid, nt); break;
+            case 17: stage_r<T, 17, cdiv(EPT, 17)>(buf, pg, N, Ns, tw, tid, nt); break;
+            default: stage_direct<T, EPT>(buf, pg, N, Ns, R, tw, tid, nt); break;
+        }
+        Ns *= R;
+    }
+}
+
+}  // namespace qpd

@@ -1,0 +1,173 @@
+"""
+Parity of the CUDA path with the reference, through the C ABI, on a B200.
+
+Tolerances (written per test):
+  * float64 (QPD_FP64): the reference's own mgpu-vs-Python bar, I rtol 1e-9 with atol 1e-12 I_max
+    (tests/test_mgpu.py:53 of the reference); q axes bit-exact.
+  * float32 (QPD_FP32, float64 phase reduction): max |dI| / I_max <= 1e-5 and relative error
+    <= 1e-3 on voxels above 1e-6 I_max; q axes bit-exact.
+"""
+
+import numpy as np
+import pytest
+
+import analytic
+from conftest import fp32_errors, golden_names, load_golden
+
+pytestmark = pytest.mark.gpu
+
+MODES = [("fp32", "fused"), ("fp64", "fused"), ("fp64", "plain"), ("fp32", "plain")]
+
+
+def run(case, precision, schedule):
+    from qpop_diffraction_b200 import diffraction
+    return diffraction(*case.args(), precision=precision, schedule=schedule)
+
+
+def assert_parity(I, ref, precision):
+    if precision == "fp64":
+        np.testing.assert_allclose(I, ref, rtol=1e-9, atol=1e-12 * ref.max())
+    else:
+        dmax, rel = fp32_errors(I, ref)
+        assert dmax <= 1e-5, dmax
+        assert rel <= 1e-3, rel
+
+
+@pytest.mark.parametrize("precision,schedule", MODES)
+@pytest.mark.parametrize("name", golden_names())
+def test_matches_reference_golden(gpu, name, precision, schedule):
+    case, ref = load_golden(name)
+    I, qx, qy, qz = run(case, precision, schedule)
+    for got, want in zip((qx, qy, qz), (ref.qx, ref.qy, ref.qz)):
+        assert np.array_equal(got, want)
+    assert I.shape == case.shape and I.dtype == np.float64
+    assert_parity(I, ref.I, precision)
+
+
+def test_device_path_equals_host_path(gpu):
+    torch = gpu
+    from qpop_diffraction_b200 import Plan, crystal_from
+    case, ref = load_golden("random_24x16x10_dense")
+    p = case.params
+    with Plan(case.shape, (p.dx, p.dy, p.dz), p.nPhase, p.nStruc) as plan:
+        plan.set_crystal(crystal_from(p, case.atoms))
+        host = plan.run_host(case.oPhase, case.oStruc, case.u, case.region)
+        dev = torch.device("cuda", 0)
+        packed = plan.pack(*(torch.from_numpy(a).to(dev) for a in (case.oPhase, case.oStruc, case.u, case.region)))
+        assert packed["wdense"] is not None  # overlapping phase fractions
+        out = plan.run_device(packed)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), host)
+
+
+def test_plan_reuse_and_second_reflection(gpu):
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    from oracle import diffraction_oracle as oracle
+    a = workloads.config2(shape=(16, 16, 104), hkl=(0, 0, 2))
+    b = workloads.config2(shape=(16, 16, 104), hkl=(1, 0, 3))
+    p = a.params
+    with Plan(a.shape, (p.dx, p.dy, p.dz), p.nPhase, p.nStruc, precision="fp64") as plan:
+        out = {}
+        for case in (a, b, a):
+            plan.set_crystal(crystal_from(case.params, case.atoms))
+            out.setdefault(case.name, []).append(plan.run_host(case.oPhase, case.oStruc, case.u, case.region))
+        assert np.array_equal(out[a.name][0], out[a.name][1])
+        for case in (a, b):
+            ref = oracle.diffraction(*case.args())[0]
+            assert_parity(out[case.name][0], ref, "fp64")
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 1, 7), (5, 1, 1), (2, 3, 1), (64, 1, 9), (3, 37, 2), (41, 2, 3),
+                                   (8, 8, 4096)])
+def test_edge_shapes(gpu, shape):
+    """Axes of length 1, prime lengths without a specialised radix (37, 41), the longest z."""
+    from qpop_diffraction_b200 import workloads
+    from oracle import diffraction_oracle as oracle
+    case = workloads.random_case(shape, seed=sum(shape), nPhase=1, weights="region")
+    ref = oracle.diffraction(*case.args())[0]
+    for precision in ("fp64", "fp32"):
+        I = run(case, precision, "fused")[0]
+        assert_parity(I, ref, precision)
+
+
+def test_nothing_scatters(gpu):
+    """All weights zero: every voxel is the 1e-50 floor, as in the reference (src/python/diffraction.py:111)."""
+    from qpop_diffraction_b200 import workloads
+    case = workloads.random_case((6, 5, 4), seed=3)
+    case.region = np.zeros_like(case.region)
+    for precision in ("fp32", "fp64"):
+        I = run(case, precision, "fused")[0]
+        assert np.all(I == 1e-50)
+
+
+def test_errors_are_exceptions_not_aborts(gpu):
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads, _native
+    case = workloads.random_case((6, 5, 4), seed=3)
+    p = case.params
+    with Plan(case.shape, (p.dx, p.dy, p.dz), 1) as plan:
+        with pytest.raises(RuntimeError):
+            plan.run_host(case.oPhase, case.oStruc, case.u, case.region)   # no crystal yet
+        plan.set_crystal(crystal_from(p, case.atoms))
+        with pytest.raises(ValueError):
+            plan.run_host(case.oPhase[:-1], case.oStruc, case.u, case.region)
+    with pytest.raises(ValueError):
+        Plan((4, 4, 5000), (1, 1, 1), 1)          # z longer than the z stage handles
+    with pytest.raises(ValueError):
+        Plan((4, 4, 4), (1, 1, 1), 9)             # more phases than the packed layout holds
+    with Plan(case.shape, (p.dx, p.dy, p.dz), 1, hbm_budget=4096) as plan:
+        with pytest.raises(MemoryError):
+            plan.set_crystal(crystal_from(p, case.atoms))
+    with pytest.raises(_native.QpdError):
+        Plan(case.shape, (p.dx, p.dy, p.dz), 1, device=1 << 20)
+
+
+# ---------------- the reference's analytic known answers on the GPU ----------------
+
+def ours(precision):
+    from qpop_diffraction_b200 import diffraction
+
+    def call(*args):
+        return diffraction(*args, precision=precision)
+    return call
+
+
+@pytest.mark.parametrize("hkl", analytic.REFLECTIONS, ids=lambda h: "".join(map(str, h)))
+@pytest.mark.parametrize("variant", list(analytic.VARIANTS))
+def test_structure_factor(gpu, variant, hkl):
+    analytic.check_structure_factor(ours("fp64"), variant, hkl)
+    analytic.check_structure_factor(ours("fp32"), variant, hkl, rtol=1e-5)
+
+
+def test_variant_symmetry(gpu):
+    analytic.check_variant_symmetry(ours("fp64"))
+    analytic.check_variant_symmetry(ours("fp32"), rtol=1e-5)
+
+
+@pytest.mark.parametrize("variant", ["c+", "a1+", "a2+"])
+def test_spontaneous_strain(gpu, variant):
+    analytic.check_spontaneous_strain(ours("fp64"), variant)
+    analytic.check_spontaneous_strain(ours("fp32"), variant)
+
+
+@pytest.mark.parametrize("p", [8, 16])
+@pytest.mark.parametrize("t", [8, 16])
+def test_thickness_fringes(gpu, t, p):
+    analytic.check_thickness_fringes(ours("fp64"), t, p)
+    # float32: fringes to the fp32 contract, zeros below the float32 noise floor
+    analytic.check_thickness_fringes(ours("fp32"), t, p, rtol=1e-3, zero=1e-9)
+
+
+@pytest.mark.parametrize("p", [8, 16])
+@pytest.mark.parametrize("t", [8, 16])
+def test_domain_satellites(gpu, t, p):
+    analytic.check_domain_satellites(ours("fp64"), t, p)
+    analytic.check_domain_satellites(ours("fp32"), t, p, zero=1e-9)
+
+
+def test_planted_signals(gpu):
+    for precision, ratio in (("fp64", 1e6), ("fp32", 1e3)):
+        f = ours(precision)
+        analytic.check_uniform_p_peaks_at_g(f)
+        analytic.check_uz_ramp_shifts_peak(f)
+        analytic.check_stripe_satellites_along_x_only(f, ratio=ratio)
+        analytic.check_phase_and_region_weights(f, rtol=1e-6 if precision == "fp64" else 1e-5)
