@@ -104,13 +104,13 @@ QPD_API int qpd_run_host(qpd_ctx* ctx, const double* oPhase, const double* oStru
  * *flags receives bit 0 (a cell has several phases: repack dense) and bit 1 (a weight differs
  * from 0 and 1: keep the weight array).  Replaces the scale / columns preparation of
  * src/heffte/qpop_diffraction_mgpu.cu:96,137 for data that is already on the GPU.
- * stream is a cudaStream_t (NULL: the context's stream); the call synchronises it. */
+ * stream is a cudaStream_t (NULL: the legacy default stream); the call synchronises it. */
 QPD_API int qpd_pack_device(qpd_ctx* ctx, const double* oPhase, const double* oStruc, const double* u, const double* region,
                     void* P, void* U, int8_t* phase, void* weight, void* wdense, int32_t dense, uint32_t* flags,
                     void* stream);
 
-/* The hot path on device-resident packed inputs, asynchronous on `stream` (NULL: the
- * context's stream): P, U, weight, wdense in the plan precision (weight NULL: 1; wdense
+/* The hot path on device-resident packed inputs, asynchronous on `stream` (a cudaStream_t;
+ * NULL: the legacy default stream): P, U, weight, wdense in the plan precision (weight NULL: 1; wdense
  * non-NULL selects dense mode and phase/weight are ignored); I_dev receives n float64.
  * Replaces source / fft.forward / accumulate / intensity of
  * src/heffte/qpop_diffraction_mgpu.cu:169-186. */

@@ -7,11 +7,14 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "qpopdiff.h"
+#include "qpd_fast.cuh"
 #include "qpd_kernels.cuh"
 
 using namespace qpd;
@@ -64,6 +67,9 @@ struct qpd_ctx {
     DevMem stage;   // host path, float64 staging
     DevMem Idev;    // host path, intensity
     DevMem flags;
+
+    // compile-time specialised kernels where an instantiation covers the axis (QPOP_B200_GENERIC=1 disables)
+    bool fast = true;
 
     // per-kernel timing
     bool timing = false;
@@ -565,6 +571,75 @@ template <typename T> struct Impl {
         return fail(c, QPD_ERR_UNSUPPORTED, "an axis of length %d is too long in this precision", a.N);
     }
 
+    // ---------------- compile-time specialised kernels ----------------
+    template <int NZ, int M, int NT, class RAD> static int fast_z_(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
+        constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+        a.M = M;
+        a.ps = PS;
+        const size_t smem = sizeof(C) * 4 * M * PS + sizeof(AtomPhase<T>) * a.in.nPhase * a.nAtom + 16;
+        QPD_TRY(set_smem(c, zstage_fast<T, NZ, M, NT, RAD>, smem));
+        const int64_t grid = (a.ncols + M - 1) / M;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        zstage_fast<T, NZ, M, NT, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_ZSTAGE, st, t0);
+    }
+
+    // Returns QPD_OK and sets *done when an instantiation covers nz.
+    static int fast_z(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st, bool* done) {
+        *done = true;
+        constexpr bool F = sizeof(T) == 4;
+        switch (a.nz) {
+            case 32: return fast_z_<32, F ? 32 : 16, 256, Radix<8, 4>>(c, a, st);
+            case 64: return fast_z_<64, F ? 16 : 8, 256, Radix<8, 8>>(c, a, st);
+            case 68: return fast_z_<68, F ? 12 : 6, 256, Radix<4, 17>>(c, a, st);
+            case 104: return fast_z_<104, F ? 8 : 4, 256, Radix<8, 13>>(c, a, st);
+            case 128: return fast_z_<128, F ? 8 : 4, 256, Radix<8, 4, 4>>(c, a, st);
+        }
+        *done = false;
+        return QPD_OK;
+    }
+
+    template <int N, int CZ, int NT, int VEC, bool EPI, class RAD>
+    static int fast_axis_(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        a.Cz = CZ;
+        a.nzc = (a.nz + CZ - 1) / CZ;
+        const size_t smem = sizeof(C) * N * CZ + 16;
+        QPD_TRY(set_smem(c, axis_fast<T, N, CZ, NT, VEC, EPI, RAD>, smem));
+        const int64_t grid = nouter * a.nzc;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        axis_fast<T, N, CZ, NT, VEC, EPI, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, kind, st, t0);
+    }
+
+    // float: z chunks of 8 complex64 (64-byte rows), 16-byte accesses when nz is even;
+    // double: chunks of 4 complex128 (64-byte rows).
+    template <int N, int NT, bool EPI, class RAD>
+    static int fast_axis_n(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        if constexpr (sizeof(T) == 4) {
+            if (a.nz % 2 == 0) return fast_axis_<N, 8, NT, 2, EPI, RAD>(c, a, nouter, kind, st);
+            return fast_axis_<N, 8, NT, 1, EPI, RAD>(c, a, nouter, kind, st);
+        } else {
+            return fast_axis_<N, 4, NT, 1, EPI, RAD>(c, a, nouter, kind, st);
+        }
+    }
+
+    template <bool EPI> static int fast_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st,
+                                            bool* done) {
+        *done = true;
+        switch (a.N) {
+            case 32: return fast_axis_n<32, 128, EPI, Radix<8, 4>>(c, a, nouter, kind, st);
+            case 64: return fast_axis_n<64, 128, EPI, Radix<8, 8>>(c, a, nouter, kind, st);
+            case 128: return fast_axis_n<128, 128, EPI, Radix<8, 4, 4>>(c, a, nouter, kind, st);
+            case 256: return fast_axis_n<256, 256, EPI, Radix<8, 8, 4>>(c, a, nouter, kind, st);
+            case 512: return fast_axis_n<512, 512, EPI, Radix<8, 8, 8>>(c, a, nouter, kind, st);
+            case 1024: return fast_axis_n<1024, 1024, EPI, Radix<8, 8, 4, 4>>(c, a, nouter, kind, st);
+        }
+        *done = false;
+        return QPD_OK;
+    }
+
     static Inputs<T> inputs(qpd_ctx* c, const void* P, const void* U, const int8_t* phase, const void* weight,
                             const void* wdense) {
         Inputs<T> in;
@@ -597,7 +672,9 @@ template <typename T> struct Impl {
             z.fstride = n;
             for (int d = 0; d < 3; d++) z.tq[d] = c->tq[d];
             z.zp = axis_plan(c, 2);
-            QPD_TRY(run_z(c, z, st));
+            bool done = false;
+            if (c->fast) QPD_TRY(fast_z(c, z, st, &done));
+            if (!done) QPD_TRY(run_z(c, z, st));
 
             AxisArgs<T> y;
             std::memset(&y, 0, sizeof y);
@@ -611,7 +688,9 @@ template <typename T> struct Impl {
             y.segs = tab<Segment<T>>(c, c->off_segY);
             y.nseg = c->nsegY;
             y.ap = axis_plan(c, 1);
-            QPD_TRY(run_axis<false>(c, y, c->nx, QPD_K_YPASS, st));
+            done = false;
+            if (c->fast) QPD_TRY(fast_axis<false>(c, y, c->nx, QPD_K_YPASS, st, &done));
+            if (!done) QPD_TRY(run_axis<false>(c, y, c->nx, QPD_K_YPASS, st));
 
             AxisArgs<T> x;
             std::memset(&x, 0, sizeof x);
@@ -629,6 +708,9 @@ template <typename T> struct Impl {
             x.scale2 = c->scale2;
             x.nx = c->nx;
             x.ny = c->ny;
+            done = false;
+            if (c->fast) QPD_TRY(fast_axis<true>(c, x, c->ny, QPD_K_XPASS, st, &done));
+            if (done) return QPD_OK;
             return run_axis<true>(c, x, c->ny, QPD_K_XPASS, st);
         }
         // plain schedule
@@ -825,6 +907,29 @@ int upload_twiddles(qpd_ctx* c, int d, int64_t N) {
     return QPD_OK;
 }
 
+// The butterflies' unit roots, once per device (constant memory is per device and module).
+int roots_init(qpd_ctx* c) {
+    static std::mutex mu;
+    static std::vector<char> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)done.size() <= c->device) done.resize(c->device + 1, 0);
+    if (done[c->device]) return QPD_OK;
+    double2 rd[kRootsTotal];
+    float2 rf[kRootsTotal];
+    for (int R : kOddRadices) {
+        const int off = root_offset(R);
+        for (int m = 0; m < R; m++) {
+            const double a = 2.0 * M_PI * (double)m / (double)R;
+            rd[off + m] = make_double2(std::cos(a), -std::sin(a));
+            rf[off + m] = make_float2((float)rd[off + m].x, (float)rd[off + m].y);
+        }
+    }
+    QPD_CU(c, cudaMemcpyToSymbol(c_roots_d, rd, sizeof rd));
+    QPD_CU(c, cudaMemcpyToSymbol(c_roots_f, rf, sizeof rf));
+    done[c->device] = 1;
+    return QPD_OK;
+}
+
 int use_device(qpd_ctx* c) {
     QPD_CU(c, cudaSetDevice(c->device));
     return QPD_OK;
@@ -846,10 +951,19 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     qpd_ctx* c = new qpd_ctx();
     c->device = device;
     c->budget = hbm_budget_bytes;
+    const char* gen = std::getenv("QPOP_B200_GENERIC");
+    c->fast = !(gen && gen[0] == '1');
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete c;
         return fail(nullptr, QPD_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    const int r = roots_init(c);
+    if (r != QPD_OK) {
+        g_create_error = c->err;
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return r;
     }
     *out = c;
     return QPD_OK;
@@ -954,7 +1068,7 @@ int qpd_pack_device(qpd_ctx* c, const double* oPhase, const double* oStruc, cons
     if (dense ? !wdense : (!phase || !weight)) return fail(c, QPD_ERR_ARG, "qpd_pack_device: NULL weight output");
     QPD_TRY(use_device(c));
     QPD_TRY(dev_reserve(c, c->flags, 256, "flags"));
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t n = c->n;
     const double* ost[3] = {nullptr, nullptr, nullptr};
     const double* uu[3];
@@ -981,7 +1095,7 @@ int qpd_run_device(qpd_ctx* c, const void* P, const void* U, const int8_t* phase
     if (!c->planned || !c->have_crystal) return fail(c, QPD_ERR_STATE, "qpd_run_device needs qpd_plan and qpd_set_crystal");
     if (!P || !U || !I_dev || (!wdense && !phase)) return fail(c, QPD_ERR_ARG, "qpd_run_device: NULL array");
     QPD_TRY(use_device(c));
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (c->precision == QPD_FP64) {
         Inputs<double> in = Impl<double>::inputs(c, P, U, phase, weight, wdense);
         return Impl<double>::run_device(c, in, I_dev, st);

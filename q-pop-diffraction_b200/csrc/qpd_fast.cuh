@@ -1,0 +1,245 @@
+// Compile-time specialised fused kernels for the axis lengths of the measured workloads.
+//
+// Same work as zstage_kernel / axis_kernel in qpd_kernels.cuh, with the axis length, its radix
+// stages, the tile shape and the thread count fixed at compile time: index arithmetic folds to
+// shifts and multiplies, register arrays are sized exactly, and global accesses move two
+// complex64 values (16 bytes) per thread when the z extent is even.  qpd_api.cu picks these
+// kernels when a plan's axis lengths have an instantiation and falls back to the generic ones.
+#pragma once
+
+#include "qpd_kernels.cuh"
+
+namespace qpd {
+
+// ---------------------------------------------------------------------------------------
+// z stage: source + FFT along z + fold, M columns of NZ cells per CTA
+// ---------------------------------------------------------------------------------------
+template <typename T, int NZ, int M, int NT, class RAD>
+__global__ void __launch_bounds__(NT) zstage_fast(ZArgs<T> a) {
+    using C = C_t<T>;
+    constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+    constexpr int PLANE = M * PS;
+    constexpr int CELLS = M * NZ;
+    constexpr int CPT = cdiv(CELLS, NT);
+    using GE = Geo<4 * M, 4 * M, PS, 0, 1, NT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(buf + 4 * PLANE);
+    const int tid = threadIdx.x;
+    const int nap = a.in.nPhase * a.nAtom;
+    for (int i = tid; i < nap; i += NT) apc[i] = a.apc[i];
+
+    const long long c0 = (long long)blockIdx.x * M;
+    const int ncell = (int)min((long long)M, a.ncols - c0) * NZ;
+    const long long g0 = c0 * NZ;
+    const C* tw = static_cast<const C*>(a.zp.tw);
+
+    CellIn<T> cell[CPT];
+    int ph[CPT];
+    T wt[CPT];
+    C accE[CPT], accX[CPT], accY[CPT];
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int e = tid + q * NT;
+        accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+        ph[q] = -1;
+        wt[q] = T(0);
+        if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+            const long long g = g0 + e;
+            load_cell<T>(a.in, g, a.tq, cell[q]);
+            if (!a.in.wdense) {
+                ph[q] = a.in.phase[g];
+                wt[q] = a.in.weight ? a.in.weight[g] : T(1);
+            }
+        }
+    }
+    __syncthreads();
+
+    for (int at = 0; at < a.nAtom; at++) {
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                const int m = e / NZ;
+                const int s = m * PS + (e - m * NZ);
+                C E, X, Y, Z;
+                cell_source<T>(a.in, g0 + e, cell[q], ph[q], wt[q], apc, a.nAtom, at, E, X, Y, Z);
+                buf[s] = E;
+                buf[PLANE + s] = X;
+                buf[2 * PLANE + s] = Y;
+                buf[3 * PLANE + s] = Z;
+            }
+        }
+        __syncthreads();
+        fft_ct<T, NZ, GE>(buf, tw, tid, RAD{});
+        const C* ce = a.coefE + (long long)at * NZ;
+        const C* cu = a.coefUz + (long long)at * NZ;
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                const int m = e / NZ;
+                const int kz = e - m * NZ;
+                const int s = m * PS + kz;
+                const C e1 = ce[kz], u1 = cu[kz];
+                cfma(accE[q], e1, buf[s]);
+                cfma(accE[q], u1, buf[3 * PLANE + s]);
+                cfma(accX[q], e1, buf[PLANE + s]);
+                cfma(accY[q], e1, buf[2 * PLANE + s]);
+            }
+        }
+        const int g = a.grp[at];
+        if (at == a.nAtom - 1 || a.grp[at + 1] != g) {
+            C* o = a.out + 3LL * g * a.fstride + g0;
+#pragma unroll
+            for (int q = 0; q < CPT; q++) {
+                const int e = tid + q * NT;
+                if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                    o[e] = accE[q];
+                    o[a.fstride + e] = accX[q];
+                    o[2 * a.fstride + e] = accY[q];
+                }
+                accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Strided axis pass on an N x CZ tile (rows along the axis, CZ contiguous z values).
+// VEC complex values per global access (2: 16-byte float4 for complex64 when nz is even).
+// ---------------------------------------------------------------------------------------
+template <typename T, int N, int CZ, int NT, int VEC, bool EPI, class RAD>
+__global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
+    using C = C_t<T>;
+    static_assert(CZ % VEC == 0, "chunk must hold whole vectors");
+    constexpr int GROUPS = N * CZ / VEC;          // vector slots in the tile
+    constexpr int EP = cdiv(GROUPS, NT);          // slots per thread
+    constexpr int CV = CZ / VEC;                  // slots per row
+    using GE = Geo<CZ, CZ, 1, 0, CZ, NT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const int tid = threadIdx.x;
+    const long long outer = blockIdx.x / a.nzc;
+    const int z0 = (int)(blockIdx.x % a.nzc) * CZ;
+    const int cz = min(CZ, a.nz - z0);
+    const long long base = outer * a.ostride + z0;
+    const C* tw = static_cast<const C*>(a.ap.tw);
+
+    for (int sg = 0; sg < a.nseg; sg++) {
+        const Segment<T>& seg = a.segs[sg];
+        C acc[2][EP][VEC];
+#pragma unroll
+        for (int q = 0; q < EP; q++)
+#pragma unroll
+            for (int w = 0; w < VEC; w++) acc[0][q][w] = acc[1][q][w] = cmake<C>(0, 0);
+        for (int fi = 0; fi < seg.nin; fi++) {
+            const C* src = a.in + seg.in[fi] * a.fstride + base;
+#pragma unroll
+            for (int q = 0; q < EP; q++) {
+                const int e = tid + q * NT;
+                if (GROUPS % NT == 0 || e < GROUPS) {
+                    const int i = e / CV;
+                    const int c = (e - i * CV) * VEC;
+                    C* d = buf + i * CZ + c;
+                    if (c < cz) {
+                        if constexpr (VEC == 2) {
+                            const float4 v = *reinterpret_cast<const float4*>(src + i * a.stride + c);
+                            *reinterpret_cast<float4*>(d) = v;
+                        } else {
+                            d[0] = src[i * a.stride + c];
+                        }
+                    } else {
+#pragma unroll
+                        for (int w = 0; w < VEC; w++) d[w] = cmake<C>(0, 0);
+                    }
+                }
+            }
+            __syncthreads();
+            fft_ct<T, N, GE>(buf, tw, tid, RAD{});
+#pragma unroll
+            for (int o = 0; o < 2; o++) {
+                if (o >= seg.nout) break;
+                const C* cf = seg.coef[o][fi];
+                const bool mine = seg.ident ? (fi == o) : (cf != nullptr);
+                if (!mine) continue;
+#pragma unroll
+                for (int q = 0; q < EP; q++) {
+                    const int e = tid + q * NT;
+                    if (GROUPS % NT == 0 || e < GROUPS) {
+                        const int k = e / CV;
+                        const int c = (e - k * CV) * VEC;
+                        const C* s = buf + k * CZ + c;
+                        if (seg.ident) {
+#pragma unroll
+                            for (int w = 0; w < VEC; w++) acc[o][q][w] = cadd(acc[o][q][w], s[w]);
+                        } else {
+                            const C f = cf[k];
+#pragma unroll
+                            for (int w = 0; w < VEC; w++) cfma(acc[o][q][w], f, s[w]);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (EPI) {
+            const long long ky = outer;
+            const long long sy = (ky + a.ny / 2) % a.ny;
+            const double syv = a.S[1][ky];
+#pragma unroll
+            for (int q = 0; q < EP; q++) {
+                const int e = tid + q * NT;
+                if (GROUPS % NT == 0 || e < GROUPS) {
+                    const int kx = e / CV;
+                    const int c = (e - kx * CV) * VEC;
+                    const double sxy = a.S[0][kx] * syv;
+                    const long long row = ((kx + a.nx / 2) % a.nx * a.ny + sy) * a.nz;
+#pragma unroll
+                    for (int w = 0; w < VEC; w++) {
+                        const int kz = z0 + c + w;
+                        if (c + w < cz) {
+                            const double S = sxy * a.S[2][kz];
+                            const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
+                            const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
+                            a.I[row + (kz + a.nz / 2) % a.nz] = v;
+                        }
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int o = 0; o < 2; o++) {
+                if (o >= seg.nout) break;
+                C* dst = a.out + seg.out[o] * a.fstride + base;
+#pragma unroll
+                for (int q = 0; q < EP; q++) {
+                    const int e = tid + q * NT;
+                    if (GROUPS % NT == 0 || e < GROUPS) {
+                        const int i = e / CV;
+                        const int c = (e - i * CV) * VEC;
+                        if (c < cz) {
+                            C* d = dst + i * a.stride + c;
+                            C v[VEC];
+#pragma unroll
+                            for (int w = 0; w < VEC; w++) v[w] = acc[o][q][w];
+                            if (a.accumulate) {
+#pragma unroll
+                                for (int w = 0; w < VEC; w++) v[w] = cadd(v[w], d[w]);
+                            }
+                            if constexpr (VEC == 2) {
+                                *reinterpret_cast<float4*>(d) = *reinterpret_cast<const float4*>(v);
+                            } else {
+                                d[0] = v[0];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace qpd

@@ -11,6 +11,7 @@
 #pragma once
 
 #include "qpd_common.cuh"
+#include "qpd_roots.cuh"
 
 namespace qpd {
 
@@ -39,9 +40,10 @@ struct Pencils {
 
 template <int R, typename C> struct Dft {
     // Odd R: pair r with R - r, y[s] = x0 + sum_r (cos a_r - i sin b_r), y[R - s] = x0 + sum_r (cos a_r + i sin b_r),
-    // with a_r = x_r + x_{R-r}, b_r = x_r - x_{R-r}, angles 2 pi r s / R; w[m] = exp(-2 pi i m / R).
-    __device__ __forceinline__ static void run(C (&x)[R], const C (&w)[R]) {
-        static_assert(R % 2 == 1, "generic radix must be odd");
+    // with a_r = x_r + x_{R-r}, b_r = x_r - x_{R-r}, angles 2 pi r s / R; the roots come from constant memory.
+    __device__ __forceinline__ static void run(C (&x)[R]) {
+        static_assert(R % 2 == 1 && root_offset(R) >= 0, "odd radix without a root table");
+        using T = decltype(C::x);
         constexpr int H = (R - 1) / 2;
         C a[H], b[H];
 #pragma unroll
@@ -58,9 +60,9 @@ template <int R, typename C> struct Dft {
             C B = cmake<C>(0, 0);
 #pragma unroll
             for (int r = 1; r <= H; r++) {
-                const int m = (r * s) % R;
-                const auto c = w[m].x;
-                const auto sn = -w[m].y;
+                const C w = unit_root<T>(root_offset(R) + (r * s) % R);
+                const T c = w.x;
+                const T sn = -w.y;
                 A.x = fma(c, a[r - 1].x, A.x);
                 A.y = fma(c, a[r - 1].y, A.y);
                 B.x = fma(sn, b[r - 1].x, B.x);
@@ -74,7 +76,7 @@ template <int R, typename C> struct Dft {
 };
 
 template <typename C> struct Dft<2, C> {
-    __device__ __forceinline__ static void run(C (&x)[2], const C (&)[2]) {
+    __device__ __forceinline__ static void run(C (&x)[2]) {
         C a = x[0];
         x[0] = cadd(a, x[1]);
         x[1] = csub(a, x[1]);
@@ -82,7 +84,7 @@ template <typename C> struct Dft<2, C> {
 };
 
 template <typename C> struct Dft<3, C> {
-    __device__ __forceinline__ static void run(C (&x)[3], const C (&)[3]) {
+    __device__ __forceinline__ static void run(C (&x)[3]) {
         using R_t = decltype(C::x);
         const R_t h = R_t(0.86602540378443864676);  // sqrt(3) / 2
         C t = cadd(x[1], x[2]);
@@ -103,11 +105,11 @@ template <typename C> __device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, 
 }
 
 template <typename C> struct Dft<4, C> {
-    __device__ __forceinline__ static void run(C (&x)[4], const C (&)[4]) { dft4(x[0], x[1], x[2], x[3]); }
+    __device__ __forceinline__ static void run(C (&x)[4]) { dft4(x[0], x[1], x[2], x[3]); }
 };
 
 template <typename C> struct Dft<8, C> {
-    __device__ __forceinline__ static void run(C (&x)[8], const C (&)[8]) {
+    __device__ __forceinline__ static void run(C (&x)[8]) {
         using R_t = decltype(C::x);
         const R_t r2 = R_t(0.70710678118654752440);  // 1 / sqrt(2)
         C e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
@@ -128,8 +130,6 @@ template <typename C> struct Dft<8, C> {
     }
 };
 
-template <int R> __host__ __device__ constexpr bool generic_radix() { return R != 2 && R != 3 && R != 4 && R != 8; }
-
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 
 // One radix-R stage over all pencils of the tile, in place.  BPT bounds the butterflies
@@ -141,11 +141,6 @@ __device__ __forceinline__ void stage_r(C_t<T>* buf, const Pencils& pg, int N, i
     const int L = N / R;
     const int nb = pg.count * L;
     const int tstep = N / (Ns * R);
-    C w[R];
-    if constexpr (generic_radix<R>()) {
-#pragma unroll
-        for (int m = 0; m < R; m++) w[m] = tw[m * L];
-    }
     C v[BPT][R];
     int ob[BPT];
 #pragma unroll
@@ -162,7 +157,7 @@ __device__ __forceinline__ void stage_r(C_t<T>* buf, const Pencils& pg, int N, i
 #pragma unroll
                 for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], tw[r * k * tstep]);
             }
-            Dft<R, C>::run(v[q], w);
+            Dft<R, C>::run(v[q]);
             ob[q] = pb + ((j / Ns) * Ns * R + k) * pg.estride;
         }
     }
@@ -247,6 +242,70 @@ __device__ void fft_pencils(C_t<T>* buf, const Pencils& pg, const AxisPlan& ap, 
         }
         Ns *= R;
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// Compile-time FFT: the axis length, the radices and the tile geometry are template
+// parameters, so index arithmetic folds to constants and register arrays are exact.
+// ---------------------------------------------------------------------------------------
+
+// Tile geometry: COUNT pencils, pencil pc at (pc % G) * PSTR + (pc / G) * GSTR, elements ES apart,
+// NT threads.
+template <int COUNT_, int G_, int PSTR_, int GSTR_, int ES_, int NT_> struct Geo {
+    static constexpr int COUNT = COUNT_, G = G_, PSTR = PSTR_, GSTR = GSTR_, ES = ES_, NT = NT_;
+    __device__ __forceinline__ static int base(int pc) { return (pc % G) * PSTR + (pc / G) * GSTR; }
+};
+
+template <typename T, int N, int NS, int R, class GE>
+__device__ __forceinline__ void stage_ct(C_t<T>* buf, const C_t<T>* __restrict__ tw, int t) {
+    using C = C_t<T>;
+    constexpr int L = N / R;
+    constexpr int NB = GE::COUNT * L;
+    constexpr int BPT = cdiv(NB, GE::NT);
+    constexpr int TSTEP = N / (NS * R);
+    C v[BPT][R];
+    int ob[BPT];
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const int b = t + q * GE::NT;
+        if (NB % GE::NT == 0 || b < NB) {
+            const int pc = b % GE::COUNT;
+            const int j = b / GE::COUNT;
+            const int k = j % NS;
+            const int pb = GE::base(pc);
+#pragma unroll
+            for (int r = 0; r < R; r++) v[q][r] = buf[pb + (j + r * L) * GE::ES];
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], tw[r * k * TSTEP]);
+            }
+            Dft<R, C>::run(v[q]);
+            ob[q] = pb + ((j / NS) * NS * R + k) * GE::ES;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const int b = t + q * GE::NT;
+        if (NB % GE::NT == 0 || b < NB) {
+#pragma unroll
+            for (int r = 0; r < R; r++) buf[ob[q] + r * NS * GE::ES] = v[q][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int... Rs> struct Radix {};
+
+template <typename T, int N, int NS, class GE, int R, int... Rest>
+__device__ __forceinline__ void fft_ct_(C_t<T>* buf, const C_t<T>* __restrict__ tw, int t) {
+    stage_ct<T, N, NS, R, GE>(buf, tw, t);
+    if constexpr (sizeof...(Rest) > 0) fft_ct_<T, N, NS * R, GE, Rest...>(buf, tw, t);
+}
+
+template <typename T, int N, class GE, int... Rs>
+__device__ __forceinline__ void fft_ct(C_t<T>* buf, const C_t<T>* __restrict__ tw, int t, Radix<Rs...>) {
+    if constexpr (sizeof...(Rs) > 0) fft_ct_<T, N, 1, GE, Rs...>(buf, tw, t);
 }
 
 }  // namespace qpd

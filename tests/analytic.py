@@ -246,7 +246,7 @@ def check_stripe_satellites_along_x_only(diffraction, ratio=1e6):
     assert on_x > ratio * on_y
 
 
-def check_phase_and_region_weights(diffraction, rtol=1e-6):
+def check_phase_and_region_weights(diffraction, rtol=1e-6, lit=1e-20):
     """Weight = phase fraction x region: uniform 0.6, 0.5 scale I by 0.3^2; a half region halves the amplitude
     (tests/test_planted.py:206-219)."""
     P = np.zeros((3,) + PLANTED)
@@ -259,6 +259,6 @@ def check_phase_and_region_weights(diffraction, rtol=1e-6):
     halved, *_ = diffraction(*run_case(P, u, q00, region=half))
     # Above the 1e-50 floor only: for these uniform fields the reference's own FFT returns exact zeros
     # off the Bragg peak, so floored voxels are 1e-50 in both runs and cannot scale by 0.09.
-    lit = plain > 1e-20 * plain.max()
-    np.testing.assert_allclose(uniform[lit], 0.09 * plain[lit], rtol=rtol)
+    mask = plain > lit * plain.max()
+    np.testing.assert_allclose(uniform[mask], 0.09 * plain[mask], rtol=rtol)
     np.testing.assert_allclose(at(halved, axes, (0.0, 0.0, G002)), 0.25 * at(plain, axes, (0.0, 0.0, G002)), rtol=rtol)

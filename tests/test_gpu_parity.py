@@ -77,17 +77,46 @@ def test_plan_reuse_and_second_reflection(gpu):
             assert_parity(out[case.name][0], ref, "fp64")
 
 
-@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 1, 7), (5, 1, 1), (2, 3, 1), (64, 1, 9), (3, 37, 2), (41, 2, 3),
-                                   (8, 8, 4096)])
-def test_edge_shapes(gpu, shape):
-    """Axes of length 1, prime lengths without a specialised radix (37, 41), the longest z."""
+@pytest.mark.parametrize("shape,precisions", [
+    ((1, 1, 1), ("fp64", "fp32")), ((1, 1, 7), ("fp64", "fp32")), ((5, 1, 1), ("fp64", "fp32")),
+    ((2, 3, 1), ("fp64", "fp32")), ((64, 1, 9), ("fp64", "fp32")), ((3, 37, 2), ("fp64", "fp32")),
+    ((41, 2, 3), ("fp64", "fp32")), ((4, 4, 2048), ("fp64", "fp32")), ((2, 2, 4096), ("fp32",))])
+def test_edge_shapes(gpu, shape, precisions):
+    """Axes of length 1, prime lengths without a specialised radix (37, 41), the longest z per precision."""
     from qpop_diffraction_b200 import workloads
     from oracle import diffraction_oracle as oracle
     case = workloads.random_case(shape, seed=sum(shape), nPhase=1, weights="region")
     ref = oracle.diffraction(*case.args())[0]
-    for precision in ("fp64", "fp32"):
+    for precision in precisions:
         I = run(case, precision, "fused")[0]
         assert_parity(I, ref, precision)
+
+
+@pytest.mark.parametrize("shape", [(512, 2, 104), (2, 512, 104), (256, 128, 64), (128, 256, 68), (1024, 2, 32),
+                                   (2, 1024, 128), (32, 64, 128), (64, 32, 32), (512, 2, 7), (2, 256, 9)])
+def test_specialised_axis_lengths(gpu, shape):
+    """Every axis length with a compile-time kernel, in both strided positions, even and odd nz."""
+    from qpop_diffraction_b200 import workloads
+    from oracle import diffraction_oracle as oracle
+    case = workloads.random_case(shape, seed=sum(shape) + 7, nPhase=2, weights="onehot", strain=True)
+    ref = oracle.diffraction(*case.args())[0]
+    for precision in ("fp32", "fp64"):
+        assert_parity(run(case, precision, "fused")[0], ref, precision)
+
+
+def test_specialised_equals_generic(gpu, monkeypatch):
+    """The compile-time kernels and the generic ones compute the same volume (QPOP_B200_GENERIC=1)."""
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    case = workloads.config2(shape=(64, 64, 104), hkl=(1, 0, 3))
+    p = case.params
+    out = []
+    for generic in ("0", "1"):
+        monkeypatch.setenv("QPOP_B200_GENERIC", generic)
+        with Plan(case.shape, (p.dx, p.dy, p.dz), p.nPhase, p.nStruc) as plan:
+            plan.set_crystal(crystal_from(p, case.atoms))
+            out.append(plan.run_host(case.oPhase, case.oStruc, case.u, case.region))
+    dmax = np.abs(out[0] - out[1]).max() / out[1].max()
+    assert dmax <= 1e-6, dmax
 
 
 def test_nothing_scatters(gpu):
@@ -170,4 +199,7 @@ def test_planted_signals(gpu):
         analytic.check_uniform_p_peaks_at_g(f)
         analytic.check_uz_ramp_shifts_peak(f)
         analytic.check_stripe_satellites_along_x_only(f, ratio=ratio)
-        analytic.check_phase_and_region_weights(f, rtol=1e-6 if precision == "fp64" else 1e-5)
+        if precision == "fp64":
+            analytic.check_phase_and_region_weights(f)
+        else:  # float32: voxels above its noise floor
+            analytic.check_phase_and_region_weights(f, rtol=1e-5, lit=1e-6)
