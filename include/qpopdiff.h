@@ -117,6 +117,11 @@ QPD_API int qpd_pack_device(qpd_ctx* ctx, const double* oPhase, const double* oS
 QPD_API int qpd_run_device(qpd_ctx* ctx, const void* P, const void* U, const int8_t* phase, const void* weight,
                    const void* wdense, double* I_dev, void* stream);
 
+/* Wait for the device and report whether a kernel of this context gave up on a bounded wait
+ * (a tile load that never completed): QPD_OK, or QPD_ERR_CUDA with the status cleared.
+ * qpd_run_host checks this itself; callers of qpd_run_device call it after synchronising. */
+QPD_API int qpd_device_status(qpd_ctx* ctx);
+
 /* Device bytes the context holds, and kernels it has launched since creation. */
 QPD_API uint64_t qpd_workspace_bytes(const qpd_ctx* ctx);
 QPD_API uint64_t qpd_launch_count(const qpd_ctx* ctx);

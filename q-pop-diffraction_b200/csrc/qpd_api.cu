@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "qpopdiff.h"
 #include "qpd_fast.cuh"
 #include "qpd_kernels.cuh"
@@ -67,6 +69,8 @@ struct qpd_ctx {
     DevMem stage;   // host path, float64 staging
     DevMem Idev;    // host path, intensity
     DevMem flags;
+    DevMem status;  // device status word of the bounded waits (QPD_DEVERR_*)
+    bool tma = true;  // TMA-fed kernels where the layout allows (QPOP_B200_NO_TMA=1 disables)
 
     // compile-time specialised kernels where an instantiation covers the axis (QPOP_B200_GENERIC=1 disables)
     bool fast = true;
@@ -106,6 +110,10 @@ int fail(qpd_ctx* c, int code, const char* fmt, ...) {
         int r_ = (expr);       \
         if (r_ != QPD_OK) return r_; \
     } while (0)
+
+int check_status(qpd_ctx* c);
+int field_map(qpd_ctx* c, CUtensorMap* m, void* base, bool fp64, int64_t nz, int64_t ny, int64_t nfx, int bz, int by,
+              int bx);
 
 int dev_free(qpd_ctx* c, DevMem& m) {
     if (m.p) {
@@ -585,10 +593,32 @@ template <typename T> struct Impl {
         return tstop(c, QPD_K_ZSTAGE, st, t0);
     }
 
+    template <int NZ, int M, int NT, class RAD> static int smem_z_(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
+        constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+        a.M = M;
+        a.ps = PS;
+        const size_t smem = zstage_smem_bytes<T, NZ, M>(a.in.nPhase * a.nAtom);
+        QPD_TRY(set_smem(c, zstage_smem<T, NZ, M, NT, RAD>, smem));
+        const int64_t grid = (a.ncols + M - 1) / M;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        zstage_smem<T, NZ, M, NT, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_ZSTAGE, st, t0);
+    }
+
     // Returns QPD_OK and sets *done when an instantiation covers nz.
     static int fast_z(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st, bool* done) {
         *done = true;
         constexpr bool F = sizeof(T) == 4;
+        if (c->tma) {
+            switch (a.nz) {
+                case 32: return smem_z_<32, F ? 32 : 16, F ? 512 : 256, Radix<8, 4>>(c, a, st);
+                case 64: return smem_z_<64, F ? 16 : 8, F ? 512 : 256, Radix<8, 8>>(c, a, st);
+                case 68: return smem_z_<68, F ? 12 : 6, F ? 416 : 224, Radix<4, 17>>(c, a, st);
+                case 104: return smem_z_<104, F ? 8 : 4, F ? 416 : 224, Radix<8, 13>>(c, a, st);
+                case 128: return smem_z_<128, F ? 8 : 4, F ? 512 : 256, Radix<8, 4, 4>>(c, a, st);
+            }
+        }
         switch (a.nz) {
             case 32: return fast_z_<32, F ? 32 : 16, 256, Radix<8, 4>>(c, a, st);
             case 64: return fast_z_<64, F ? 16 : 8, 256, Radix<8, 8>>(c, a, st);
@@ -613,10 +643,40 @@ template <typename T> struct Impl {
         return tstop(c, kind, st, t0);
     }
 
+    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD>
+    static int tma_axis_(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        constexpr int BOX = N > 256 ? 256 : N;
+        a.Cz = CZ;
+        a.nzc = (a.nz + CZ - 1) / CZ;
+        CUtensorMap map;
+        const int64_t nfields = c->sched_used == QPD_SCHED_FUSED ? 3 * c->ng1 : 2;
+        QPD_TRY(field_map(c, &map, const_cast<C*>(a.in), sizeof(T) == 8, a.nz, c->ny, nfields * c->nx, 2 * CZ,
+                          XP ? 1 : BOX, XP ? BOX : 1));
+        const size_t smem = sizeof(C) * N * CZ * 2 + 128;
+        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD>, smem));
+        const int64_t grid = nouter * a.nzc;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD><<<(unsigned)grid, NT, smem, st>>>(map, a);
+        return tstop(c, kind, st, t0);
+    }
+
     // float: z chunks of 8 complex64 (64-byte rows), 16-byte accesses when nz is even;
     // double: chunks of 4 complex128 (64-byte rows).
     template <int N, int NT, bool EPI, class RAD>
     static int fast_axis_n(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        // TMA: the map's row strides must be multiples of 16 bytes (nz even for complex64)
+        const bool tma_ok = c->tma && (sizeof(T) == 8 || a.nz % 2 == 0);
+        if (tma_ok) {
+            const bool xp = kind == QPD_K_XPASS || (kind == QPD_K_AXIS && a.stride != a.nz);
+            if constexpr (sizeof(T) == 4) {
+                if (xp) return tma_axis_<N, 8, NT, 2, EPI, true, RAD>(c, a, nouter, kind, st);
+                return tma_axis_<N, 8, NT, 2, EPI, false, RAD>(c, a, nouter, kind, st);
+            } else {
+                if (xp) return tma_axis_<N, 4, NT, 1, EPI, true, RAD>(c, a, nouter, kind, st);
+                return tma_axis_<N, 4, NT, 1, EPI, false, RAD>(c, a, nouter, kind, st);
+            }
+        }
         if constexpr (sizeof(T) == 4) {
             if (a.nz % 2 == 0) return fast_axis_<N, 8, NT, 2, EPI, RAD>(c, a, nouter, kind, st);
             return fast_axis_<N, 8, NT, 1, EPI, RAD>(c, a, nouter, kind, st);
@@ -672,6 +732,7 @@ template <typename T> struct Impl {
             z.fstride = n;
             for (int d = 0; d < 3; d++) z.tq[d] = c->tq[d];
             z.zp = axis_plan(c, 2);
+            z.status = static_cast<int*>(c->status.p);
             bool done = false;
             if (c->fast) QPD_TRY(fast_z(c, z, st, &done));
             if (!done) QPD_TRY(run_z(c, z, st));
@@ -688,6 +749,9 @@ template <typename T> struct Impl {
             y.segs = tab<Segment<T>>(c, c->off_segY);
             y.nseg = c->nsegY;
             y.ap = axis_plan(c, 1);
+            y.nx = c->nx;
+            y.ny = c->ny;
+            y.status = static_cast<int*>(c->status.p);
             done = false;
             if (c->fast) QPD_TRY(fast_axis<false>(c, y, c->nx, QPD_K_YPASS, st, &done));
             if (!done) QPD_TRY(run_axis<false>(c, y, c->nx, QPD_K_YPASS, st));
@@ -708,6 +772,7 @@ template <typename T> struct Impl {
             x.scale2 = c->scale2;
             x.nx = c->nx;
             x.ny = c->ny;
+            x.status = static_cast<int*>(c->status.p);
             done = false;
             if (c->fast) QPD_TRY(fast_axis<true>(c, x, c->ny, QPD_K_XPASS, st, &done));
             if (done) return QPD_OK;
@@ -755,6 +820,9 @@ template <typename T> struct Impl {
                     ax.segs = tab<Segment<T>>(c, c->off_segX);
                     ax.nseg = 1;
                     ax.ap = axis_plan(c, d);
+                    ax.nx = c->nx;
+                    ax.ny = c->ny;
+                    ax.status = static_cast<int*>(c->status.p);
                     QPD_TRY(run_axis<false>(c, ax, d == 1 ? c->nx : c->ny, QPD_K_AXIS, st));
                 }
 
@@ -885,7 +953,7 @@ template <typename T> struct Impl {
         QPD_TRY(run_device(c, in, Id, st));
         QPD_CU(c, cudaMemcpyAsync(I, Id, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
         QPD_CU(c, cudaStreamSynchronize(st));
-        return QPD_OK;
+        return check_status(c);
     }
 };
 
@@ -930,8 +998,47 @@ int roots_init(qpd_ctx* c) {
     return QPD_OK;
 }
 
+// Read and clear the device status word; a recorded timeout becomes QPD_ERR_CUDA.
+int check_status(qpd_ctx* c) {
+    int v = 0;
+    QPD_CU(c, cudaMemcpy(&v, c->status.p, sizeof v, cudaMemcpyDeviceToHost));
+    if (v == 0) return QPD_OK;
+    QPD_CU(c, cudaMemset(c->status.p, 0, sizeof v));
+    return fail(c, QPD_ERR_CUDA, "a kernel gave up waiting for its tile loads (device status %d)", v);
+}
+
 int use_device(qpd_ctx* c) {
     QPD_CU(c, cudaSetDevice(c->device));
+    return QPD_OK;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Tensor map over a field array viewed as (2 nz reals, ny, nfields * nx), box (bz, by, bx).
+int field_map(qpd_ctx* c, CUtensorMap* m, void* base, bool fp64, int64_t nz, int64_t ny, int64_t nfx, int bz, int by,
+              int bx) {
+    auto fn = encode_fn();
+    if (!fn) return fail(c, QPD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t esz = fp64 ? 8 : 4;
+    cuuint64_t dims[3] = {(cuuint64_t)(2 * nz), (cuuint64_t)ny, (cuuint64_t)nfx};
+    cuuint64_t strides[2] = {(cuuint64_t)(2 * nz) * esz, (cuuint64_t)(2 * nz * ny) * esz};
+    cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)by, (cuuint32_t)bx};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(m, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides,
+                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(c, QPD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return QPD_OK;
 }
 
@@ -953,12 +1060,16 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     c->budget = hbm_budget_bytes;
     const char* gen = std::getenv("QPOP_B200_GENERIC");
     c->fast = !(gen && gen[0] == '1');
+    const char* notma = std::getenv("QPOP_B200_NO_TMA");
+    c->tma = !(notma && notma[0] == '1');
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete c;
         return fail(nullptr, QPD_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
     }
-    const int r = roots_init(c);
+    int r = roots_init(c);
+    if (r == QPD_OK) r = dev_reserve(c, c->status, 256, "status word");
+    if (r == QPD_OK && cudaMemset(c->status.p, 0, 256) != cudaSuccess) r = fail(c, QPD_ERR_CUDA, "cudaMemset failed");
     if (r != QPD_OK) {
         g_create_error = c->err;
         cudaStreamDestroy(c->stream);
@@ -974,7 +1085,7 @@ int qpd_destroy(qpd_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (DevMem* m : {&c->tw[0], &c->tw[1], &c->tw[2], &c->tables, &c->fields, &c->packed, &c->dense, &c->stage,
-                      &c->Idev, &c->flags})
+                      &c->Idev, &c->flags, &c->status})
         dev_free(c, *m);
     for (auto& r : c->recs) {
         cudaEventDestroy(r.a);
@@ -1130,6 +1241,12 @@ int qpd_stage_times(qpd_ctx* c, double* ms, uint64_t* counts, int32_t cap) {
     }
     c->recs.clear();
     return rc;
+}
+
+int qpd_device_status(qpd_ctx* c) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_device_status: ctx is NULL");
+    QPD_TRY(use_device(c));
+    return check_status(c);
 }
 
 uint64_t qpd_workspace_bytes(const qpd_ctx* c) { return c ? c->held : 0; }

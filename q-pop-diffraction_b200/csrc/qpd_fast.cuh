@@ -8,6 +8,7 @@
 #pragma once
 
 #include "qpd_kernels.cuh"
+#include "qpd_tma.cuh"
 
 namespace qpd {
 
@@ -240,6 +241,323 @@ __global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
         }
         __syncthreads();
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// Strided axis pass with TMA: the N x CZ tile of every input field arrives by
+// cp.async.bulk.tensor into one of two shared-memory buffers, the next field's load in flight
+// while the current one is transformed and folded.  The tensor map views the field array as
+// (2 nz reals, ny, nfields * nx); XPASS selects rows along x (box 2CZ x 1 x BOX) instead of
+// along y (box 2CZ x BOX x 1).  Out-of-range z of a partial chunk arrives as zeros.
+// ---------------------------------------------------------------------------------------
+template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD>
+__global__ void __launch_bounds__(NT) axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
+    using C = C_t<T>;
+    static_assert(CZ % VEC == 0, "chunk must hold whole vectors");
+    constexpr int NO = EPI ? 1 : 2;
+    constexpr int TILE = N * CZ;
+    constexpr int GROUPS = TILE / VEC;
+    constexpr int EP = cdiv(GROUPS, NT);
+    constexpr int CV = CZ / VEC;
+    constexpr int BOX = N > 256 ? 256 : N;
+    static_assert(N % BOX == 0, "rows must split into whole boxes");
+    constexpr uint32_t BYTES = TILE * sizeof(C);
+    using GE = Geo<CZ, CZ, 1, 0, CZ, NT>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    C* bufs = reinterpret_cast<C*>(smem_raw);
+    __shared__ __align__(8) uint64_t bar[2];
+    const int tid = threadIdx.x;
+    const long long outer = blockIdx.x / a.nzc;
+    const int z0 = (int)(blockIdx.x % a.nzc) * CZ;
+    const int cz = min(CZ, a.nz - z0);
+    const long long base = outer * a.ostride + z0;
+    const C* tw = static_cast<const C*>(a.ap.tw);
+    const int nfx = (int)(XPASS ? a.nx : a.nx);  // rows of one field in the map's outer dimension: nx
+
+    int total = 0;
+    for (int sg = 0; sg < a.nseg; sg++) total += a.segs[sg].nin;
+
+    // field of the flat input index fl
+    auto field_of = [&](int fl) {
+        for (int sg = 0; sg < a.nseg; sg++) {
+            const int k = a.segs[sg].nin;
+            if (fl < k) return a.segs[sg].in[fl];
+            fl -= k;
+        }
+        return 0;
+    };
+    auto issue = [&](int fl, int b) {
+        const int f = field_of(fl);
+        C* dst = bufs + b * TILE;
+        mbar_expect_tx(&bar[b], BYTES);
+#pragma unroll
+        for (int k = 0; k < N / BOX; k++) {
+            if (XPASS) tma_load_3d(dst + k * BOX * CZ, &map, &bar[b], 2 * z0, (int)outer, f * nfx + k * BOX);
+            else tma_load_3d(dst + k * BOX * CZ, &map, &bar[b], 2 * z0, k * BOX, f * nfx + (int)outer);
+        }
+    };
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (total > 0) issue(0, 0);
+        if (total > 1) issue(1, 1);
+    }
+
+    int fl = 0;
+    for (int sg = 0; sg < a.nseg; sg++) {
+        const Segment<T>& seg = a.segs[sg];
+        C acc[NO][EP][VEC];
+#pragma unroll
+        for (int o = 0; o < NO; o++)
+#pragma unroll
+            for (int q = 0; q < EP; q++)
+#pragma unroll
+                for (int w = 0; w < VEC; w++) acc[o][q][w] = cmake<C>(0, 0);
+        for (int fi = 0; fi < seg.nin; fi++, fl++) {
+            const int b = fl & 1;
+            C* buf = bufs + b * TILE;
+            const bool ok = mbar_wait(&bar[b], (fl >> 1) & 1, a.status);
+            if (!__syncthreads_and(ok)) {
+                // a load never completed: give the other buffer's load a bounded chance to land, then stop
+                if (tid == 0 && fl + 1 < total) mbar_wait(&bar[b ^ 1], ((fl + 1) >> 1) & 1, nullptr);
+                return;
+            }
+            fft_ct<T, N, GE>(buf, tw, tid, RAD{});
+#pragma unroll
+            for (int o = 0; o < NO; o++) {
+                if (o >= seg.nout) break;
+                const C* cf = seg.coef[o][fi];
+                const bool mine = seg.ident ? (fi == o) : (cf != nullptr);
+                if (!mine) continue;
+#pragma unroll
+                for (int q = 0; q < EP; q++) {
+                    const int e = tid + q * NT;
+                    if (GROUPS % NT == 0 || e < GROUPS) {
+                        const int k = e / CV;
+                        const int c = (e - k * CV) * VEC;
+                        const C* s = buf + k * CZ + c;
+                        if (seg.ident) {
+#pragma unroll
+                            for (int w = 0; w < VEC; w++) acc[o][q][w] = cadd(acc[o][q][w], s[w]);
+                        } else {
+                            const C f = cf[k];
+#pragma unroll
+                            for (int w = 0; w < VEC; w++) cfma(acc[o][q][w], f, s[w]);
+                        }
+                    }
+                }
+            }
+            __syncthreads();  // buffer b free again
+            if (tid == 0 && fl + 2 < total) {
+                fence_proxy_async();
+                issue(fl + 2, b);
+            }
+        }
+        if (EPI) {
+            const long long ky = outer;
+            const long long sy = (ky + a.ny / 2) % a.ny;
+            const double syv = a.S[1][ky];
+#pragma unroll
+            for (int q = 0; q < EP; q++) {
+                const int e = tid + q * NT;
+                if (GROUPS % NT == 0 || e < GROUPS) {
+                    const int kx = e / CV;
+                    const int c = (e - kx * CV) * VEC;
+                    const double sxy = a.S[0][kx] * syv;
+                    const long long row = ((kx + a.nx / 2) % a.nx * a.ny + sy) * a.nz;
+#pragma unroll
+                    for (int w = 0; w < VEC; w++) {
+                        const int kz = z0 + c + w;
+                        if (c + w < cz) {
+                            const double S = sxy * a.S[2][kz];
+                            const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
+                            const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
+                            a.I[row + (kz + a.nz / 2) % a.nz] = v;
+                        }
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int o = 0; o < NO; o++) {
+                if (o >= seg.nout) break;
+                C* dst = a.out + seg.out[o] * a.fstride + base;
+#pragma unroll
+                for (int q = 0; q < EP; q++) {
+                    const int e = tid + q * NT;
+                    if (GROUPS % NT == 0 || e < GROUPS) {
+                        const int i = e / CV;
+                        const int c = (e - i * CV) * VEC;
+                        if (c < cz) {
+                            C* d = dst + i * a.stride + c;
+                            C v[VEC];
+#pragma unroll
+                            for (int w = 0; w < VEC; w++) v[w] = acc[o][q][w];
+                            if (a.accumulate) {
+#pragma unroll
+                                for (int w = 0; w < VEC; w++) v[w] = cadd(v[w], d[w]);
+                            }
+                            if constexpr (VEC == 2) {
+                                *reinterpret_cast<float4*>(d) = *reinterpret_cast<const float4*>(v);
+                            } else {
+                                d[0] = v[0];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// z stage with the tile's inputs in shared memory: P, U (and the phase index / weight)
+// arrive by 1-D bulk copies, tu = qC . u / (2 pi) is formed once per cell; each thread keeps
+// only its cells' accumulators in registers.  NT threads, CPT cells per thread.
+// ---------------------------------------------------------------------------------------
+template <typename T, int NZ, int M, int NT, class RAD>
+__global__ void __launch_bounds__(NT, 2) zstage_smem(ZArgs<T> a) {
+    using C = C_t<T>;
+    constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+    constexpr int PLANE = M * PS;
+    constexpr int CELLS = M * NZ;
+    constexpr int CPT = cdiv(CELLS, NT);
+    constexpr int CELLS16 = (CELLS + 15) / 16 * 16;
+    using GE = Geo<4 * M, 4 * M, PS, 0, 1, NT>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // layout: buf (4 PLANE complex) | in (6 CELLS T) | wt (CELLS T) | tu (CELLS double) | ph (CELLS16 int8) | apc
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    T* sin_ = reinterpret_cast<T*>(buf + 4 * PLANE);
+    T* swt = sin_ + 6 * CELLS;
+    double* stu = reinterpret_cast<double*>(swt + CELLS + (CELLS % 2));
+    signed char* sph = reinterpret_cast<signed char*>(stu + CELLS);
+    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(sph + CELLS16);
+    __shared__ __align__(8) uint64_t bar;
+    const int tid = threadIdx.x;
+    const int nap = a.in.nPhase * a.nAtom;
+    for (int i = tid; i < nap; i += NT) apc[i] = a.apc[i];
+
+    const long long c0 = (long long)blockIdx.x * M;
+    const int ncell = (int)min((long long)M, a.ncols - c0) * NZ;
+    const long long g0 = c0 * NZ;
+    const C* tw = static_cast<const C*>(a.zp.tw);
+    const bool single = a.in.wdense == nullptr;
+    const bool bulk = (ncell * sizeof(T)) % 16 == 0 && (g0 * sizeof(T)) % 16 == 0 && (a.in.n * sizeof(T)) % 16 == 0 &&
+                      (!single || (ncell % 16 == 0 && g0 % 16 == 0)) && a.in.nStruc == 3;
+    if (bulk) {
+        if (tid == 0) {
+            mbar_init(&bar, 1);
+            fence_barrier_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t pb = ncell * sizeof(T);
+            uint32_t bytes = 6 * pb + (single ? ncell + (a.in.weight ? pb : 0) : 0);
+            mbar_expect_tx(&bar, bytes);
+            for (int k = 0; k < 3; k++) {
+                bulk_load(sin_ + k * CELLS, a.in.P + k * a.in.n + g0, pb, &bar);
+                bulk_load(sin_ + (3 + k) * CELLS, a.in.U + k * a.in.n + g0, pb, &bar);
+            }
+            if (single) {
+                bulk_load(sph, a.in.phase + g0, ncell, &bar);
+                if (a.in.weight) bulk_load(swt, a.in.weight + g0, pb, &bar);
+            }
+        }
+        const bool ok = mbar_wait(&bar, 0, a.status);
+        if (!__syncthreads_and(ok)) return;
+    } else {
+        for (int e = tid; e < ncell; e += NT) {
+            for (int k = 0; k < 3; k++) {
+                sin_[k * CELLS + e] = k < a.in.nStruc ? a.in.P[k * a.in.n + g0 + e] : T(0);
+                sin_[(3 + k) * CELLS + e] = a.in.U[k * a.in.n + g0 + e];
+            }
+            if (single) {
+                sph[e] = a.in.phase[g0 + e];
+                if (a.in.weight) swt[e] = a.in.weight[g0 + e];
+            }
+        }
+    }
+    for (int e = tid; e < ncell; e += NT) {
+        stu[e] = a.tq[0] * (double)sin_[3 * CELLS + e] + a.tq[1] * (double)sin_[4 * CELLS + e] +
+                 a.tq[2] * (double)sin_[5 * CELLS + e];
+        if (single && !a.in.weight) swt[e] = T(1);
+    }
+    __syncthreads();
+
+    C accE[CPT], accX[CPT], accY[CPT];
+#pragma unroll
+    for (int q = 0; q < CPT; q++) accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+
+    for (int at = 0; at < a.nAtom; at++) {
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                CellIn<T> cl;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    cl.p[k] = sin_[k * CELLS + e];
+                    cl.u[k] = sin_[(3 + k) * CELLS + e];
+                }
+                cl.tu = stu[e];
+                const int m = e / NZ;
+                const int s = m * PS + (e - m * NZ);
+                C E, X, Y, Z;
+                cell_source<T>(a.in, g0 + e, cl, single ? (int)sph[e] : -1, single ? swt[e] : T(0), apc, a.nAtom,
+                               at, E, X, Y, Z);
+                buf[s] = E;
+                buf[PLANE + s] = X;
+                buf[2 * PLANE + s] = Y;
+                buf[3 * PLANE + s] = Z;
+            }
+        }
+        __syncthreads();
+        fft_ct<T, NZ, GE>(buf, tw, tid, RAD{});
+        const C* ce = a.coefE + (long long)at * NZ;
+        const C* cu = a.coefUz + (long long)at * NZ;
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                const int m = e / NZ;
+                const int kz = e - m * NZ;
+                const int s = m * PS + kz;
+                const C e1 = ce[kz], u1 = cu[kz];
+                cfma(accE[q], e1, buf[s]);
+                cfma(accE[q], u1, buf[3 * PLANE + s]);
+                cfma(accX[q], e1, buf[PLANE + s]);
+                cfma(accY[q], e1, buf[2 * PLANE + s]);
+            }
+        }
+        const int g = a.grp[at];
+        if (at == a.nAtom - 1 || a.grp[at + 1] != g) {
+            C* o = a.out + 3LL * g * a.fstride + g0;
+#pragma unroll
+            for (int q = 0; q < CPT; q++) {
+                const int e = tid + q * NT;
+                if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                    o[e] = accE[q];
+                    o[a.fstride + e] = accX[q];
+                    o[2 * a.fstride + e] = accY[q];
+                }
+                accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Shared memory of zstage_smem.
+template <typename T, int NZ, int M> constexpr size_t zstage_smem_bytes(int nap) {
+    constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+    constexpr int CELLS = M * NZ;
+    return sizeof(C_t<T>) * 4 * M * PS + sizeof(T) * (7 * CELLS + CELLS % 2) + sizeof(double) * CELLS +
+           (CELLS + 15) / 16 * 16 + sizeof(AtomPhase<T>) * nap + 16;
 }
 
 }  // namespace qpd

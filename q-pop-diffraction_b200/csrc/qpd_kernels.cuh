@@ -173,6 +173,7 @@ template <typename T> struct ZArgs {
     long long fstride;
     double tq[3];                 // qC / (2 pi)
     AxisPlan zp;
+    int* status;                  // device status word: bounded waits record timeouts here
 };
 
 template <typename T, int NT, int EPT>
@@ -295,6 +296,7 @@ template <typename T> struct AxisArgs {
     const double* S[3];
     double scale2;      // (1 / (n V))^2
     long long nx, ny;
+    int* status;        // device status word: bounded waits record timeouts here
 };
 
 template <typename T, int NT, int EPT, bool EPI>

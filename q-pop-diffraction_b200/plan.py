@@ -125,6 +125,10 @@ class Plan:
     def workspace_bytes(self):
         return int(self.lib.qpd_workspace_bytes(self._ctx))
 
+    def device_status(self):
+        """Raise if a kernel of this plan gave up on a bounded wait (reads and clears the device status)."""
+        self._check(self.lib.qpd_device_status(self._ctx))
+
     def enable_timing(self, on=True):
         """Record CUDA events around every kernel launch (see stage_times)."""
         self._check(self.lib.qpd_enable_timing(self._ctx, int(bool(on))))
