@@ -74,6 +74,10 @@ struct qpd_ctx {
 
     // compile-time specialised kernels where an instantiation covers the axis (QPOP_B200_GENERIC=1 disables)
     bool fast = true;
+    // launch-shape choices among equivalent kernels: QPOP_B200_ZCFG (z stage thread layout),
+    // QPOP_B200_NBUF (tile buffers of the TMA passes, 2 or 3)
+    int knob_z = 0;
+    int knob_nbuf = 2;
 
     // per-kernel timing
     bool timing = false;
@@ -316,7 +320,7 @@ template <typename T> struct Impl {
                 for (int g1 = 0; g1 < G1; g1++) cnt += g2of[g1] == g2;
                 maxin = std::max(maxin, 3 * cnt);
             }
-            if (A > kMaxAtoms || maxin > kMaxSegIn || 2 * G2 > kMaxSegIn || G2 > kMaxSegs) sched = QPD_SCHED_PLAIN;
+            if (A > kMaxAtoms || maxin > kMaxSegIn || 2 * G2 > kMaxSegIn || 2 * G2 > kMaxSegs) sched = QPD_SCHED_PLAIN;
         }
         c->sched_used = sched;
         c->nAtom = A;
@@ -406,25 +410,30 @@ template <typename T> struct Impl {
                 }
             }
             // segments hold device addresses: filled in once the buffer exists
+            // one output per segment: E2 <- (E1, Y1) of the g1 groups sharing R_x, then X2 <- X1.
+            // Writing E2 into slot 2 g2 before X1 of the same g2 is read is safe: X1 slots are 3 g1 + 1 > 2 g2.
             for (int g2 = 0; g2 < G2; g2++) {
-                Segment<T> s;
-                std::memset(&s, 0, sizeof s);
-                s.nout = 2;
-                s.out[0] = 2 * g2;
-                s.out[1] = 2 * g2 + 1;
-                for (int g1 = 0; g1 < G1; g1++) {
-                    if (g2of[g1] != g2) continue;
-                    for (int comp = 0; comp < 3; comp++) {
-                        s.in[s.nin] = 3 * g1 + comp;
-                        // store table offsets + 1 for now (0 = no contribution)
+                for (int out = 0; out < 2; out++) {
+                    Segment<T> s;
+                    std::memset(&s, 0, sizeof s);
+                    s.nout = 1;
+                    s.out[0] = 2 * g2 + out;
+                    for (int g1 = 0; g1 < G1; g1++) {
+                        if (g2of[g1] != g2) continue;
+                        // table offsets + 1 for now (0 = no contribution); fixed up once the buffer exists
                         const size_t e = offY[g1] + 1, mi = offY[g1] + sizeof(C) * N[1] + 1;
-                        if (comp == 0) s.coef[0][s.nin] = reinterpret_cast<const C*>(e);
-                        if (comp == 2) s.coef[0][s.nin] = reinterpret_cast<const C*>(mi);
-                        if (comp == 1) s.coef[1][s.nin] = reinterpret_cast<const C*>(e);
-                        s.nin++;
+                        if (out == 0) {
+                            s.in[s.nin] = 3 * g1 + 0;
+                            s.coef[0][s.nin++] = reinterpret_cast<const C*>(e);
+                            s.in[s.nin] = 3 * g1 + 2;
+                            s.coef[0][s.nin++] = reinterpret_cast<const C*>(mi);
+                        } else {
+                            s.in[s.nin] = 3 * g1 + 1;
+                            s.coef[0][s.nin++] = reinterpret_cast<const C*>(e);
+                        }
                     }
+                    segY.push_back(s);
                 }
-                segY.push_back(s);
             }
             Segment<T> s;
             std::memset(&s, 0, sizeof s);
@@ -436,7 +445,7 @@ template <typename T> struct Impl {
                 s.coef[0][s.nin++] = reinterpret_cast<const C*>(offX[g2] + sizeof(C) * N[0] + 1);
             }
             segX.push_back(s);
-            c->nsegY = G2;
+            c->nsegY = 2 * G2;
             c->off_segY = place(sizeof(Segment<T>) * segY.size());
             c->off_segX = place(sizeof(Segment<T>));
         } else {
@@ -594,15 +603,20 @@ template <typename T> struct Impl {
     }
 
     template <int NZ, int M, int NT, class RAD> static int smem_z_(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
-        constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+        using L = ZLayout<T, NZ, M>;
         a.M = M;
-        a.ps = PS;
-        const size_t smem = zstage_smem_bytes<T, NZ, M>(a.in.nPhase * a.nAtom);
-        QPD_TRY(set_smem(c, zstage_smem<T, NZ, M, NT, RAD>, smem));
-        const int64_t grid = (a.ncols + M - 1) / M;
+        a.ps = L::PS;
+        const size_t smem = L::bytes(a.in.nPhase * a.nAtom, a.nAtom);
+        if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "z stage tables exceed shared memory");
+        QPD_TRY(set_smem(c, zstage_pipe<T, NZ, M, NT, RAD>, smem));
+        int per_sm = 0, sms = 0;
+        QPD_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zstage_pipe<T, NZ, M, NT, RAD>, NT, smem));
+        QPD_CU(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        const int64_t ntiles = (a.ncols + M - 1) / M;
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sms));
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
-        zstage_smem<T, NZ, M, NT, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
+        zstage_pipe<T, NZ, M, NT, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
         return tstop(c, QPD_K_ZSTAGE, st, t0);
     }
 
@@ -610,12 +624,14 @@ template <typename T> struct Impl {
     static int fast_z(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st, bool* done) {
         *done = true;
         constexpr bool F = sizeof(T) == 4;
-        if (c->tma) {
+        if (c->tma && ZLayout<T, 128, 8>::bytes(a.in.nPhase * a.nAtom, a.nAtom) <= max_smem(c)) {
             switch (a.nz) {
                 case 32: return smem_z_<32, F ? 32 : 16, F ? 512 : 256, Radix<8, 4>>(c, a, st);
                 case 64: return smem_z_<64, F ? 16 : 8, F ? 512 : 256, Radix<8, 8>>(c, a, st);
-                case 68: return smem_z_<68, F ? 12 : 6, F ? 416 : 224, Radix<4, 17>>(c, a, st);
-                case 104: return smem_z_<104, F ? 8 : 4, F ? 416 : 224, Radix<8, 13>>(c, a, st);
+                case 68: return smem_z_<68, F ? 12 : 6, F ? 416 : 224, Pfa<4, 17>>(c, a, st);
+                case 104:
+                    if (F && c->knob_z == 1) return smem_z_<104, 8, 256, Pfa<8, 13>>(c, a, st);
+                    return smem_z_<104, F ? 8 : 4, F ? 416 : 224, Pfa<8, 13>>(c, a, st);
                 case 128: return smem_z_<128, F ? 8 : 4, F ? 512 : 256, Radix<8, 4, 4>>(c, a, st);
             }
         }
@@ -645,6 +661,12 @@ template <typename T> struct Impl {
 
     template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD>
     static int tma_axis_(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        if (c->knob_nbuf == 2) return tma_axis_b<N, CZ, NT, VEC, EPI, XP, RAD, 2>(c, a, nouter, kind, st);
+        return tma_axis_b<N, CZ, NT, VEC, EPI, XP, RAD, 3>(c, a, nouter, kind, st);
+    }
+
+    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF>
+    static int tma_axis_b(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
         constexpr int BOX = N > 256 ? 256 : N;
         a.Cz = CZ;
         a.nzc = (a.nz + CZ - 1) / CZ;
@@ -652,12 +674,13 @@ template <typename T> struct Impl {
         const int64_t nfields = c->sched_used == QPD_SCHED_FUSED ? 3 * c->ng1 : 2;
         QPD_TRY(field_map(c, &map, const_cast<C*>(a.in), sizeof(T) == 8, a.nz, c->ny, nfields * c->nx, 2 * CZ,
                           XP ? 1 : BOX, XP ? BOX : 1));
-        const size_t smem = sizeof(C) * N * CZ * 2 + 128;
-        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD>, smem));
+        const size_t smem = sizeof(C) * N * CZ * NBUF + sizeof(C) * N + 128;
+        if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "axis tile exceeds shared memory");
+        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF>, smem));
         const int64_t grid = nouter * a.nzc;
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
-        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD><<<(unsigned)grid, NT, smem, st>>>(map, a);
+        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF><<<(unsigned)grid, NT, smem, st>>>(map, a);
         return tstop(c, kind, st, t0);
     }
 
@@ -1062,6 +1085,8 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     c->fast = !(gen && gen[0] == '1');
     const char* notma = std::getenv("QPOP_B200_NO_TMA");
     c->tma = !(notma && notma[0] == '1');
+    if (const char* k = std::getenv("QPOP_B200_ZCFG")) c->knob_z = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_NBUF")) c->knob_nbuf = std::atoi(k) == 3 ? 3 : 2;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete c;

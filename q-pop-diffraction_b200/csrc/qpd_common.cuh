@@ -35,8 +35,5 @@ template <typename C> __device__ __forceinline__ C cmul_mi(C a) { return cmake<C
 // +i * a
 template <typename C> __device__ __forceinline__ C cmul_pi(C a) { return cmake<C>(-a.y, a.x); }
 
-template <typename T> __device__ __forceinline__ void sincospi_t(T x, T* s, T* c);
-template <> __device__ __forceinline__ void sincospi_t<float>(float x, float* s, float* c) { sincospif(x, s, c); }
-template <> __device__ __forceinline__ void sincospi_t<double>(double x, double* s, double* c) { sincospi(x, s, c); }
 
 }  // namespace qpd

@@ -250,11 +250,11 @@ __global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
 // (2 nz reals, ny, nfields * nx); XPASS selects rows along x (box 2CZ x 1 x BOX) instead of
 // along y (box 2CZ x BOX x 1).  Out-of-range z of a partial chunk arrives as zeros.
 // ---------------------------------------------------------------------------------------
-template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD>
-__global__ void __launch_bounds__(NT) axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
+template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF>
+__global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
     using C = C_t<T>;
     static_assert(CZ % VEC == 0, "chunk must hold whole vectors");
-    constexpr int NO = EPI ? 1 : 2;
+    constexpr int NO = 1;  // the host builds single-output segments for this kernel
     constexpr int TILE = N * CZ;
     constexpr int GROUPS = TILE / VEC;
     constexpr int EP = cdiv(GROUPS, NT);
@@ -265,13 +265,14 @@ __global__ void __launch_bounds__(NT) axis_tma(const __grid_constant__ CUtensorM
     using GE = Geo<CZ, CZ, 1, 0, CZ, NT>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     C* bufs = reinterpret_cast<C*>(smem_raw);
-    __shared__ __align__(8) uint64_t bar[2];
+    C* tw = bufs + NBUF * TILE;  // twiddles, N values
+    __shared__ __align__(8) uint64_t bar[NBUF];
     const int tid = threadIdx.x;
     const long long outer = blockIdx.x / a.nzc;
     const int z0 = (int)(blockIdx.x % a.nzc) * CZ;
     const int cz = min(CZ, a.nz - z0);
     const long long base = outer * a.ostride + z0;
-    const C* tw = static_cast<const C*>(a.ap.tw);
+    for (int i = tid; i < N; i += NT) tw[i] = static_cast<const C*>(a.ap.tw)[i];
     const int nfx = (int)(XPASS ? a.nx : a.nx);  // rows of one field in the map's outer dimension: nx
 
     int total = 0;
@@ -298,15 +299,12 @@ __global__ void __launch_bounds__(NT) axis_tma(const __grid_constant__ CUtensorM
     };
 
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int b = 0; b < NBUF; b++) mbar_init(&bar[b], 1);
         fence_barrier_init();
     }
     __syncthreads();
-    if (tid == 0) {
-        if (total > 0) issue(0, 0);
-        if (total > 1) issue(1, 1);
-    }
+    if (tid == 0)
+        for (int b = 0; b < NBUF && b < total; b++) issue(b, b);
 
     int fl = 0;
     for (int sg = 0; sg < a.nseg; sg++) {
@@ -319,21 +317,29 @@ __global__ void __launch_bounds__(NT) axis_tma(const __grid_constant__ CUtensorM
 #pragma unroll
                 for (int w = 0; w < VEC; w++) acc[o][q][w] = cmake<C>(0, 0);
         for (int fi = 0; fi < seg.nin; fi++, fl++) {
-            const int b = fl & 1;
+            const int b = fl % NBUF;
             C* buf = bufs + b * TILE;
-            const bool ok = mbar_wait(&bar[b], (fl >> 1) & 1, a.status);
+            // this thread's coefficients for the field, fetched before the wait
+            const C* cf = seg.coef[0][fi];
+            C cfr[EP];
+            if (!seg.ident && cf) {
+#pragma unroll
+                for (int q = 0; q < EP; q++) {
+                    const int e = tid + q * NT;
+                    cfr[q] = (GROUPS % NT == 0 || e < GROUPS) ? cf[e / CV] : cmake<C>(0, 0);
+                }
+            }
+            const bool ok = mbar_wait(&bar[b], (fl / NBUF) & 1, a.status);
             if (!__syncthreads_and(ok)) {
-                // a load never completed: give the other buffer's load a bounded chance to land, then stop
-                if (tid == 0 && fl + 1 < total) mbar_wait(&bar[b ^ 1], ((fl + 1) >> 1) & 1, nullptr);
+                // a load never completed: give the other buffers' loads a bounded chance to land, then stop
+                if (tid == 0)
+                    for (int k = 1; k < NBUF && fl + k < total; k++)
+                        mbar_wait(&bar[(fl + k) % NBUF], ((fl + k) / NBUF) & 1, nullptr);
                 return;
             }
             fft_ct<T, N, GE>(buf, tw, tid, RAD{});
-#pragma unroll
-            for (int o = 0; o < NO; o++) {
-                if (o >= seg.nout) break;
-                const C* cf = seg.coef[o][fi];
-                const bool mine = seg.ident ? (fi == o) : (cf != nullptr);
-                if (!mine) continue;
+            const bool mine = seg.ident ? (fi == 0) : (cf != nullptr);
+            if (mine) {
 #pragma unroll
                 for (int q = 0; q < EP; q++) {
                     const int e = tid + q * NT;
@@ -343,19 +349,18 @@ __global__ void __launch_bounds__(NT) axis_tma(const __grid_constant__ CUtensorM
                         const C* s = buf + k * CZ + c;
                         if (seg.ident) {
 #pragma unroll
-                            for (int w = 0; w < VEC; w++) acc[o][q][w] = cadd(acc[o][q][w], s[w]);
+                            for (int w = 0; w < VEC; w++) acc[0][q][w] = cadd(acc[0][q][w], s[w]);
                         } else {
-                            const C f = cf[k];
 #pragma unroll
-                            for (int w = 0; w < VEC; w++) cfma(acc[o][q][w], f, s[w]);
+                            for (int w = 0; w < VEC; w++) cfma(acc[0][q][w], cfr[q], s[w]);
                         }
                     }
                 }
             }
             __syncthreads();  // buffer b free again
-            if (tid == 0 && fl + 2 < total) {
+            if (tid == 0 && fl + NBUF < total) {
                 fence_proxy_async();
-                issue(fl + 2, b);
+                issue(fl + NBUF, b);
             }
         }
         if (EPI) {
@@ -416,148 +421,212 @@ __global__ void __launch_bounds__(NT) axis_tma(const __grid_constant__ CUtensorM
 }
 
 // ---------------------------------------------------------------------------------------
-// z stage with the tile's inputs in shared memory: P, U (and the phase index / weight)
-// arrive by 1-D bulk copies, tu = qC . u / (2 pi) is formed once per cell; each thread keeps
-// only its cells' accumulators in registers.  NT threads, CPT cells per thread.
+// z stage, persistent and pipelined: each CTA walks tiles of M columns (blockIdx.x, + gridDim.x,
+// ...).  A tile's inputs (P, U, the phase index and weight) arrive in one of two shared-memory
+// buffers by 1-D bulk copies issued a tile ahead, so the loads of tile i+1 overlap the source
+// evaluation, the z transforms and the fold of tile i.  Each thread keeps only its cells'
+// accumulators in registers.  A tile whose planes are not 16-byte aligned (only a partial last
+// tile can be) is loaded by the threads instead.
 // ---------------------------------------------------------------------------------------
+template <typename T, int NZ, int M> struct ZLayout {
+    static constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+    static constexpr int PLANE = M * PS;
+    static constexpr int CELLS = M * NZ;
+    static constexpr int CELLS16 = (CELLS + 15) / 16 * 16;
+    // one input buffer: P, U (6 CELLS T) | weight (CELLS T) | phase (CELLS16 int8), 16-byte multiple
+    static constexpr size_t INB = (sizeof(T) * 7 * CELLS + CELLS16 + 15) / 16 * 16;
+    static constexpr size_t BUF = sizeof(C_t<T>) * 4 * PLANE;
+    static constexpr size_t bytes(int nap, int nAtom) {
+        return BUF + 2 * INB + sizeof(double) * CELLS + sizeof(C_t<T>) * NZ + sizeof(AtomPhase<T>) * nap +
+               sizeof(C_t<T>) * 2 * nAtom * NZ + 64;
+    }
+};
+
 template <typename T, int NZ, int M, int NT, class RAD>
-__global__ void __launch_bounds__(NT, 2) zstage_smem(ZArgs<T> a) {
+__global__ void __launch_bounds__(NT, 2) zstage_pipe(ZArgs<T> a) {
     using C = C_t<T>;
-    constexpr int PS = NZ % 2 ? NZ : NZ + 1;
-    constexpr int PLANE = M * PS;
-    constexpr int CELLS = M * NZ;
+    using L = ZLayout<T, NZ, M>;
+    constexpr int PS = L::PS, PLANE = L::PLANE, CELLS = L::CELLS;
     constexpr int CPT = cdiv(CELLS, NT);
-    constexpr int CELLS16 = (CELLS + 15) / 16 * 16;
     using GE = Geo<4 * M, 4 * M, PS, 0, 1, NT>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // layout: buf (4 PLANE complex) | in (6 CELLS T) | wt (CELLS T) | tu (CELLS double) | ph (CELLS16 int8) | apc
     C* buf = reinterpret_cast<C*>(smem_raw);
-    T* sin_ = reinterpret_cast<T*>(buf + 4 * PLANE);
-    T* swt = sin_ + 6 * CELLS;
-    double* stu = reinterpret_cast<double*>(swt + CELLS + (CELLS % 2));
-    signed char* sph = reinterpret_cast<signed char*>(stu + CELLS);
-    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(sph + CELLS16);
-    __shared__ __align__(8) uint64_t bar;
+    unsigned char* inb = smem_raw + L::BUF;  // two input buffers of L::INB bytes
+    double* stu = reinterpret_cast<double*>(inb + 2 * L::INB);
+    C* stw = reinterpret_cast<C*>(stu + CELLS);
+    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(stw + NZ);
+    C* sce = reinterpret_cast<C*>(apc + a.in.nPhase * a.nAtom);  // [at][kz] exp(-i (k_z + G_z) R_z)
+    C* scu = sce + a.nAtom * NZ;                                  // [at][kz] -i k_z times that
+    __shared__ __align__(8) uint64_t bar[2];
     const int tid = threadIdx.x;
     const int nap = a.in.nPhase * a.nAtom;
     for (int i = tid; i < nap; i += NT) apc[i] = a.apc[i];
-
-    const long long c0 = (long long)blockIdx.x * M;
-    const int ncell = (int)min((long long)M, a.ncols - c0) * NZ;
-    const long long g0 = c0 * NZ;
-    const C* tw = static_cast<const C*>(a.zp.tw);
-    const bool single = a.in.wdense == nullptr;
-    const bool bulk = (ncell * sizeof(T)) % 16 == 0 && (g0 * sizeof(T)) % 16 == 0 && (a.in.n * sizeof(T)) % 16 == 0 &&
-                      (!single || (ncell % 16 == 0 && g0 % 16 == 0)) && a.in.nStruc == 3;
-    if (bulk) {
-        if (tid == 0) {
-            mbar_init(&bar, 1);
-            fence_barrier_init();
-        }
-        __syncthreads();
-        if (tid == 0) {
-            const uint32_t pb = ncell * sizeof(T);
-            uint32_t bytes = 6 * pb + (single ? ncell + (a.in.weight ? pb : 0) : 0);
-            mbar_expect_tx(&bar, bytes);
-            for (int k = 0; k < 3; k++) {
-                bulk_load(sin_ + k * CELLS, a.in.P + k * a.in.n + g0, pb, &bar);
-                bulk_load(sin_ + (3 + k) * CELLS, a.in.U + k * a.in.n + g0, pb, &bar);
-            }
-            if (single) {
-                bulk_load(sph, a.in.phase + g0, ncell, &bar);
-                if (a.in.weight) bulk_load(swt, a.in.weight + g0, pb, &bar);
-            }
-        }
-        const bool ok = mbar_wait(&bar, 0, a.status);
-        if (!__syncthreads_and(ok)) return;
-    } else {
-        for (int e = tid; e < ncell; e += NT) {
-            for (int k = 0; k < 3; k++) {
-                sin_[k * CELLS + e] = k < a.in.nStruc ? a.in.P[k * a.in.n + g0 + e] : T(0);
-                sin_[(3 + k) * CELLS + e] = a.in.U[k * a.in.n + g0 + e];
-            }
-            if (single) {
-                sph[e] = a.in.phase[g0 + e];
-                if (a.in.weight) swt[e] = a.in.weight[g0 + e];
-            }
-        }
+    for (int i = tid; i < NZ; i += NT) stw[i] = static_cast<const C*>(a.zp.tw)[i];
+    for (int i = tid; i < a.nAtom * NZ; i += NT) {
+        sce[i] = a.coefE[i];
+        scu[i] = a.coefUz[i];
     }
-    for (int e = tid; e < ncell; e += NT) {
-        stu[e] = a.tq[0] * (double)sin_[3 * CELLS + e] + a.tq[1] * (double)sin_[4 * CELLS + e] +
-                 a.tq[2] * (double)sin_[5 * CELLS + e];
-        if (single && !a.in.weight) swt[e] = T(1);
+
+    const bool single = a.in.wdense == nullptr;
+    const long long ntiles = (a.ncols + M - 1) / M;
+    const bool aligned = (a.in.n * sizeof(T)) % 16 == 0 && a.in.nStruc == 3 &&
+                         (reinterpret_cast<uintptr_t>(a.in.P) | reinterpret_cast<uintptr_t>(a.in.U) |
+                          reinterpret_cast<uintptr_t>(a.in.phase) | reinterpret_cast<uintptr_t>(a.in.weight)) % 16 == 0;
+    auto ncell_of = [&](long long t) { return (int)min((long long)M, a.ncols - t * M) * NZ; };
+    // Every full tile starts at a multiple of CELLS, so whether full tiles can use bulk copies is a
+    // property of the tile shape: all of a CTA's full tiles do, or none does.  That keeps the
+    // barrier phases in step with the tile count; only the partial last tile loads by threads.
+    constexpr bool TILE_BULK = (CELLS * sizeof(T)) % 16 == 0;
+    const bool bulk_mode = aligned && TILE_BULK && (!single || CELLS % 16 == 0);
+    auto bulk_ok = [&](long long t) { return bulk_mode && ncell_of(t) == CELLS; };
+    auto issue = [&](long long t, int b) {
+        const int nc = ncell_of(t);
+        const long long g0 = t * M * NZ;
+        T* sin_ = reinterpret_cast<T*>(inb + b * L::INB);
+        T* swt = sin_ + 6 * CELLS;
+        signed char* sph = reinterpret_cast<signed char*>(swt + CELLS);
+        const uint32_t pb = nc * sizeof(T);
+        mbar_expect_tx(&bar[b], 6 * pb + (single ? nc + (a.in.weight ? pb : 0) : 0));
+        for (int k = 0; k < 3; k++) {
+            bulk_load(sin_ + k * CELLS, a.in.P + k * a.in.n + g0, pb, &bar[b]);
+            bulk_load(sin_ + (3 + k) * CELLS, a.in.U + k * a.in.n + g0, pb, &bar[b]);
+        }
+        if (single) {
+            bulk_load(sph, a.in.phase + g0, nc, &bar[b]);
+            if (a.in.weight) bulk_load(swt, a.in.weight + g0, pb, &bar[b]);
+        }
+    };
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_barrier_init();
     }
     __syncthreads();
+    if (tid == 0) {
+        for (int k = 0; k < 2; k++) {
+            const long long t = blockIdx.x + (long long)k * gridDim.x;
+            if (t < ntiles && bulk_ok(t)) issue(t, k);
+        }
+    }
 
-    C accE[CPT], accX[CPT], accY[CPT];
+    // this thread's cells: source slot and output slot in the tile (atom-independent)
+    int ssrc[CPT], sout[CPT];
 #pragma unroll
-    for (int q = 0; q < CPT; q++) accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+    for (int q = 0; q < CPT; q++) {
+        const int e = tid + q * NT;
+        const int m = e / NZ;
+        const int z = e - m * NZ;
+        ssrc[q] = m * PS + z;
+        sout[q] = m * PS + OutPos<RAD>::at(z);
+    }
 
-    for (int at = 0; at < a.nAtom; at++) {
-#pragma unroll
-        for (int q = 0; q < CPT; q++) {
-            const int e = tid + q * NT;
-            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
-                CellIn<T> cl;
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    cl.p[k] = sin_[k * CELLS + e];
-                    cl.u[k] = sin_[(3 + k) * CELLS + e];
+    for (int it = 0;; it++) {
+        const long long t = blockIdx.x + (long long)it * gridDim.x;
+        if (t >= ntiles) break;
+        const int b = it & 1;
+        const int ncell = ncell_of(t);
+        const long long g0 = t * M * NZ;
+        T* sin_ = reinterpret_cast<T*>(inb + b * L::INB);
+        T* swt = sin_ + 6 * CELLS;
+        signed char* sph = reinterpret_cast<signed char*>(swt + CELLS);
+        if (bulk_ok(t)) {
+            const bool ok = mbar_wait(&bar[b], (it >> 1) & 1, a.status);
+            if (!__syncthreads_and(ok)) {
+                if (tid == 0) {
+                    const long long t2 = t + gridDim.x;
+                    if (t2 < ntiles && bulk_ok(t2)) mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, nullptr);
                 }
-                cl.tu = stu[e];
-                const int m = e / NZ;
-                const int s = m * PS + (e - m * NZ);
-                C E, X, Y, Z;
-                cell_source<T>(a.in, g0 + e, cl, single ? (int)sph[e] : -1, single ? swt[e] : T(0), apc, a.nAtom,
-                               at, E, X, Y, Z);
-                buf[s] = E;
-                buf[PLANE + s] = X;
-                buf[2 * PLANE + s] = Y;
-                buf[3 * PLANE + s] = Z;
+                return;
             }
+        } else {
+            for (int e = tid; e < ncell; e += NT) {
+                for (int k = 0; k < 3; k++) {
+                    sin_[k * CELLS + e] = k < a.in.nStruc ? a.in.P[k * a.in.n + g0 + e] : T(0);
+                    sin_[(3 + k) * CELLS + e] = a.in.U[k * a.in.n + g0 + e];
+                }
+                if (single) {
+                    sph[e] = a.in.phase[g0 + e];
+                    if (a.in.weight) swt[e] = a.in.weight[g0 + e];
+                }
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < ncell; e += NT) {
+            stu[e] = a.tq[0] * (double)sin_[3 * CELLS + e] + a.tq[1] * (double)sin_[4 * CELLS + e] +
+                     a.tq[2] * (double)sin_[5 * CELLS + e];
+            if (single && !a.in.weight) swt[e] = T(1);
         }
         __syncthreads();
-        fft_ct<T, NZ, GE>(buf, tw, tid, RAD{});
-        const C* ce = a.coefE + (long long)at * NZ;
-        const C* cu = a.coefUz + (long long)at * NZ;
+
+        C accE[CPT], accX[CPT], accY[CPT];
 #pragma unroll
-        for (int q = 0; q < CPT; q++) {
-            const int e = tid + q * NT;
-            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
-                const int m = e / NZ;
-                const int kz = e - m * NZ;
-                const int s = m * PS + kz;
-                const C e1 = ce[kz], u1 = cu[kz];
-                cfma(accE[q], e1, buf[s]);
-                cfma(accE[q], u1, buf[3 * PLANE + s]);
-                cfma(accX[q], e1, buf[PLANE + s]);
-                cfma(accY[q], e1, buf[2 * PLANE + s]);
-            }
-        }
-        const int g = a.grp[at];
-        if (at == a.nAtom - 1 || a.grp[at + 1] != g) {
-            C* o = a.out + 3LL * g * a.fstride + g0;
+        for (int q = 0; q < CPT; q++) accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+
+        for (int at = 0; at < a.nAtom; at++) {
 #pragma unroll
             for (int q = 0; q < CPT; q++) {
                 const int e = tid + q * NT;
                 if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
-                    o[e] = accE[q];
-                    o[a.fstride + e] = accX[q];
-                    o[2 * a.fstride + e] = accY[q];
+                    CellIn<T> cl;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        cl.p[k] = sin_[k * CELLS + e];
+                        cl.u[k] = sin_[(3 + k) * CELLS + e];
+                    }
+                    cl.tu = stu[e];
+                    C E, X, Y, Z;
+                    cell_source<T>(a.in, g0 + e, cl, single ? (int)sph[e] : -1, single ? swt[e] : T(0), apc,
+                                   a.nAtom, at, E, X, Y, Z);
+                    const int s = ssrc[q];
+                    buf[s] = E;
+                    buf[PLANE + s] = X;
+                    buf[2 * PLANE + s] = Y;
+                    buf[3 * PLANE + s] = Z;
                 }
-                accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+            }
+            __syncthreads();
+            fft_ct<T, NZ, GE>(buf, stw, tid, RAD{});
+            const C* ce = sce + at * NZ;
+            const C* cu = scu + at * NZ;
+#pragma unroll
+            for (int q = 0; q < CPT; q++) {
+                const int e = tid + q * NT;
+                if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                    const int kz = e % NZ;
+                    const int s = sout[q];
+                    const C e1 = ce[kz], u1 = cu[kz];
+                    cfma(accE[q], e1, buf[s]);
+                    cfma(accE[q], u1, buf[3 * PLANE + s]);
+                    cfma(accX[q], e1, buf[PLANE + s]);
+                    cfma(accY[q], e1, buf[2 * PLANE + s]);
+                }
+            }
+            const int g = a.grp[at];
+            if (at == a.nAtom - 1 || a.grp[at + 1] != g) {
+                C* o = a.out + 3LL * g * a.fstride + g0;
+#pragma unroll
+                for (int q = 0; q < CPT; q++) {
+                    const int e = tid + q * NT;
+                    if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                        o[e] = accE[q];
+                        o[a.fstride + e] = accX[q];
+                        o[2 * a.fstride + e] = accY[q];
+                    }
+                    accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+                }
+            }
+            __syncthreads();
+        }
+        // input buffer b is free: fetch the tile two steps ahead into it
+        if (tid == 0) {
+            const long long t2 = t + 2LL * gridDim.x;
+            if (t2 < ntiles && bulk_ok(t2)) {
+                fence_proxy_async();
+                issue(t2, b);
             }
         }
-        __syncthreads();
     }
-}
-
-// Shared memory of zstage_smem.
-template <typename T, int NZ, int M> constexpr size_t zstage_smem_bytes(int nap) {
-    constexpr int PS = NZ % 2 ? NZ : NZ + 1;
-    constexpr int CELLS = M * NZ;
-    return sizeof(C_t<T>) * 4 * M * PS + sizeof(T) * (7 * CELLS + CELLS % 2) + sizeof(double) * CELLS +
-           (CELLS + 15) / 16 * 16 + sizeof(AtomPhase<T>) * nap + 16;
 }
 
 }  // namespace qpd

@@ -308,4 +308,61 @@ __device__ __forceinline__ void fft_ct(C_t<T>* buf, const C_t<T>* __restrict__ t
     if constexpr (sizeof...(Rs) > 0) fft_ct_<T, N, 1, GE, Rs...>(buf, tw, t);
 }
 
+// ---------------------------------------------------------------------------------------
+// Prime-factor (Good-Thomas) FFT for N = N1 N2 with gcd(N1, N2) = 1: a 2-D DFT without twiddle
+// factors.  Input x[n] is read as A0[n1][n2] = x[(N2 n1 + N1 n2) mod N]; stage A transforms over
+// n1, stage B over n2, and X[k] ends at position (N2 (k mod N1) + N1 (k mod N2)) mod N.  Each
+// butterfly writes back exactly the positions it read, so a stage needs no barrier between its
+// loads and stores; one barrier separates the two stages.
+// ---------------------------------------------------------------------------------------
+template <int N1, int N2> struct Pfa {
+    static constexpr int N = N1 * N2;
+    // a < N1, b < N2, so N2 a + N1 b < 2 N: one conditional subtraction reduces it
+    __host__ __device__ static constexpr int pos(int a, int b) {
+        const int v = N2 * a + N1 * b;
+        return v >= N ? v - N : v;
+    }
+    // where X[k] sits after the transform
+    __host__ __device__ static constexpr int out_pos(int k) { return pos(k % N1, k % N2); }
+};
+
+template <typename T, int R, int OTHER, bool OVER_FIRST, class GE, class P>
+__device__ __forceinline__ void pfa_stage(C_t<T>* buf, int t) {
+    using C = C_t<T>;
+    constexpr int NB = GE::COUNT * OTHER;  // butterflies: one per pencil and index of the other factor
+    constexpr int BPT = cdiv(NB, GE::NT);
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const int b = t + q * GE::NT;
+        if (NB % GE::NT == 0 || b < NB) {
+            const int pc = b % GE::COUNT;
+            const int o = b / GE::COUNT;
+            const int pb = GE::base(pc);
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = buf[pb + (OVER_FIRST ? P::pos(r, o) : P::pos(o, r)) * GE::ES];
+            Dft<R, C>::run(v);
+#pragma unroll
+            for (int r = 0; r < R; r++) buf[pb + (OVER_FIRST ? P::pos(r, o) : P::pos(o, r)) * GE::ES] = v[r];
+        }
+    }
+}
+
+template <typename T, int N, class GE, int N1, int N2>
+__device__ __forceinline__ void fft_ct(C_t<T>* buf, const C_t<T>* __restrict__, int t, Pfa<N1, N2>) {
+    static_assert(N1 * N2 == N, "factors must multiply to N");
+    pfa_stage<T, N1, N2, true, GE, Pfa<N1, N2>>(buf, t);
+    __syncthreads();
+    pfa_stage<T, N2, N1, false, GE, Pfa<N1, N2>>(buf, t);
+    __syncthreads();
+}
+
+// Position of output k after fft_ct: natural order for Stockham, the CRT map for Pfa.
+template <class RAD> struct OutPos {
+    __host__ __device__ static constexpr int at(int k) { return k; }
+};
+template <int N1, int N2> struct OutPos<Pfa<N1, N2>> {
+    __host__ __device__ static constexpr int at(int k) { return Pfa<N1, N2>::out_pos(k); }
+};
+
 }  // namespace qpd

@@ -31,12 +31,18 @@ constexpr int kMaxPhases = 8;
 constexpr int kMaxSegIn = 24;
 constexpr int kMaxSegs = 32;
 
-// Per (phase, atom) constants, index p * nAtom + a (atoms in processing order).
-template <typename T> struct AtomPhase {
+// Per (phase, atom) constants, index p * nAtom + a (atoms in processing order); 16-byte
+// aligned so a thread reads one with vector loads.
+template <typename T> struct alignas(16) AtomPhase {
     double bq[3];  // sum_d qC_d su[d][k] / (2 pi): the P part of the phase, in turns
     T su[9];       // su[d * 3 + k]: shift of the atom along d per unit P_k, nm per C/m^2
     T fr, fi;      // form factor
 };
+
+// exp(-2 pi i t) for |t| <= 1/2 (already reduced in double).  float: the hardware sin / cos of an
+// argument in [-pi, pi] (absolute error about 4e-7); double: sincospi.
+__device__ __forceinline__ void expm2pi(double t, float* s, float* c) { __sincosf(6.283185307179586f * (float)t, s, c); }
+__device__ __forceinline__ void expm2pi(double t, double* s, double* c) { sincospi(2.0 * t, s, c); }
 
 // ---------------------------------------------------------------------------------------
 // Inputs
@@ -102,7 +108,7 @@ __device__ __forceinline__ void add_source(const CellIn<T>& c, const AtomPhase<T
     double t = c.tu + k.bq[0] * (double)c.p[0] + k.bq[1] * (double)c.p[1] + k.bq[2] * (double)c.p[2];
     t -= rint(t);  // reduced in double: the phase in turns, |t| <= 1/2
     T sn, cs;
-    sincospi_t<T>(T(2 * t), &sn, &cs);  // exp(-i qC . u_ap) = cs - i sn
+    expm2pi(t, &sn, &cs);  // exp(-i qC . u_ap) = cs - i sn
     const T er = w * (k.fr * cs + k.fi * sn);
     const T ei = w * (k.fi * cs - k.fr * sn);
     const T ua0 = c.u[0] + k.su[0] * c.p[0] + k.su[1] * c.p[1] + k.su[2] * c.p[2];
