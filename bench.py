@@ -68,10 +68,6 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
-
-
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -201,7 +197,8 @@ def run_reference(args, rank):
 
 def main():
     args = parse()
-    rank, world, local = dist_env()
+    from qpop_diffraction_b200 import replicas
+    rank, world, local = replicas.rank_env()
     if args.impl == "reference":
         run_reference(args, rank)
         return
@@ -273,11 +270,8 @@ def main():
             s[0] += t
             s[1] += c
         p.enable_timing(False)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps * n / (ms * 1e-3) / 1e9
+    ms = replicas.slowest(ms, dev)
+    value = replicas.throughput(args.steps * n, ms * 1e-3, world) / 1e9
 
     hbm, hbm_src = peaks()
     weight = packed["weight"] is not None
@@ -308,13 +302,9 @@ def main():
     t0 = time.perf_counter()
     for i in range(ke):
         plans[i % 2].run_host(pin_np["oPhase"], pin_np["oStruc"], pin_np["u"], pin_np["region"], out=I_host)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.slowest(time.perf_counter() - t0, dev)
     h2d = sum(a.nbytes for a in pin_np.values())
-    e2e = {"value": world * ke * n / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+    e2e = {"value": replicas.throughput(ke * n, e2e_s, world) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": I_host.nbytes, "steps": ke, "ms_per_step": e2e_s / ke * 1e3,
            "call": "qpd_run_host (float64 host arrays, pinned)"}
     for p in plans:
