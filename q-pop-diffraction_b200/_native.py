@@ -24,6 +24,7 @@ QPD_FP32 = 0
 QPD_FP64 = 1
 QPD_SCHED_FUSED = 0
 QPD_SCHED_PLAIN = 1
+QPD_NOALLOC_SCRATCH_BYTES = 32 << 20
 
 PRECISIONS = {"fp32": QPD_FP32, "fp64": QPD_FP64}
 SCHEDULES = {"fused": QPD_SCHED_FUSED, "plain": QPD_SCHED_PLAIN}
@@ -31,7 +32,7 @@ SCHEDULES = {"fused": QPD_SCHED_FUSED, "plain": QPD_SCHED_PLAIN}
 # Every symbol include/qpopdiff.h declares.
 EXPORTS = ("qpd_create", "qpd_destroy", "qpd_last_error", "qpd_plan", "qpd_set_crystal", "qpd_run_host",
            "qpd_pack_device", "qpd_run_device", "qpd_device_status", "qpd_workspace_bytes", "qpd_launch_count", "qpd_enable_timing",
-           "qpd_stage_times", "qpd_axis_radices")
+           "qpd_stage_times", "qpd_run_device_noalloc", "qpd_axis_radices")
 
 # Kernel kinds of qpd_stage_times (QPD_K_*), in index order.
 KERNEL_KINDS = ("zstage", "ypass", "xpass", "pack", "source", "fftz", "axis", "accumulate", "intensity")
@@ -92,6 +93,8 @@ def load(path=None):
         "qpd_launch_count": (c_uint64, [c_void_p]),
         "qpd_enable_timing": (c_int, [c_void_p, c_int32]),
         "qpd_stage_times": (c_int, [c_void_p, POINTER(c_double), POINTER(c_uint64), c_int32]),
+        "qpd_run_device_noalloc": (c_int, [POINTER(QpdGrid), POINTER(QpdCrystal), c_void_p, c_void_p, c_void_p,
+                                           c_void_p, c_void_p, c_void_p]),
         "qpd_axis_radices": (c_int, [c_int64, POINTER(c_int32), c_int32]),
     }
     for name, (res, args) in sig.items():

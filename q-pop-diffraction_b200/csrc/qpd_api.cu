@@ -1124,6 +1124,13 @@ int qpd_destroy(qpd_ctx* c) {
 
 const char* qpd_last_error(const qpd_ctx* c) { return c ? c->err.c_str() : g_create_error.c_str(); }
 
+}  // extern "C"
+
+// For qpd_noalloc.cu, which has no context: its failures read back through qpd_last_error(NULL).
+void qpd_internal_set_error(const char* msg) { g_create_error = msg; }
+
+extern "C" {
+
 int qpd_axis_radices(int64_t N, int32_t* radices, int32_t cap) {
     if (N < 1) return QPD_ERR_ARG;
     std::vector<int> r = factorise(N);

@@ -15,8 +15,9 @@ __host__ __device__ constexpr int root_offset(int R) {
 }
 constexpr int kRootsTotal = 3 + 5 + 7 + 11 + 13 + 17;
 
-__constant__ float2 c_roots_f[kRootsTotal];
-__constant__ double2 c_roots_d[kRootsTotal];
+// internal linkage: each translation unit that launches butterflies fills its own copy
+static __constant__ float2 c_roots_f[kRootsTotal];
+static __constant__ double2 c_roots_d[kRootsTotal];
 
 template <typename T> __device__ __forceinline__ C_t<T> unit_root(int idx);
 template <> __device__ __forceinline__ float2 unit_root<float>(int idx) { return c_roots_f[idx]; }
