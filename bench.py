@@ -292,21 +292,23 @@ def main():
 
     # ---------------- e2e: the C-ABI call with host buffers ----------------
     ke = args.e2e_steps if args.e2e_steps is not None else min(args.steps, 20)
-    pinned = {k: t.pin_memory() for k, t in host.items()}
-    pin_np = {k: t.numpy() for k, t in pinned.items()}
-    I_host = torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
-    plans[0].run_host(pin_np["oPhase"], pin_np["oStruc"], pin_np["u"], pin_np["region"], out=I_host)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for i in range(ke):
-        plans[i % 2].run_host(pin_np["oPhase"], pin_np["oStruc"], pin_np["u"], pin_np["region"], out=I_host)
-    e2e_s = replicas.slowest(time.perf_counter() - t0, dev)
-    h2d = sum(a.nbytes for a in pin_np.values())
-    e2e = {"value": replicas.throughput(ke * n, e2e_s, world) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": I_host.nbytes, "steps": ke, "ms_per_step": e2e_s / ke * 1e3,
-           "call": "qpd_run_host (float64 host arrays, pinned)"}
+    e2e = None
+    if ke > 0:
+        pinned = {k: t.pin_memory() for k, t in host.items()}
+        pin_np = {k: t.numpy() for k, t in pinned.items()}
+        I_host = torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+        plans[0].run_host(pin_np["oPhase"], pin_np["oStruc"], pin_np["u"], pin_np["region"], out=I_host)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for i in range(ke):
+            plans[i % 2].run_host(pin_np["oPhase"], pin_np["oStruc"], pin_np["u"], pin_np["region"], out=I_host)
+        e2e_s = replicas.slowest(time.perf_counter() - t0, dev)
+        h2d = sum(a.nbytes for a in pin_np.values())
+        e2e = {"value": replicas.throughput(ke * n, e2e_s, world) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": I_host.nbytes, "steps": ke, "ms_per_step": e2e_s / ke * 1e3,
+               "call": "qpd_run_host (float64 host arrays, pinned)"}
     for p in plans:
         p.close()
     del packed
