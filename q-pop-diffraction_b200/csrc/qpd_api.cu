@@ -74,7 +74,8 @@ struct qpd_ctx {
 
     // compile-time specialised kernels where an instantiation covers the axis (QPOP_B200_GENERIC=1 disables)
     bool fast = true;
-    // launch-shape choices among equivalent kernels: QPOP_B200_ZCFG (z stage thread layout),
+    // launch-shape choices among equivalent kernels: QPOP_B200_ZCFG=1 (z stage, nz = 104: 416 threads
+    // reading inputs from shared memory instead of 256 holding them in registers),
     // QPOP_B200_NBUF (tile buffers of the TMA passes, 2 or 3)
     int knob_z = 0;
     int knob_nbuf = 2;
@@ -602,21 +603,23 @@ template <typename T> struct Impl {
         return tstop(c, QPD_K_ZSTAGE, st, t0);
     }
 
-    template <int NZ, int M, int NT, class RAD> static int smem_z_(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
+    template <int NZ, int M, int NT, class RAD, bool REGIN = false>
+    static int smem_z_(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
         using L = ZLayout<T, NZ, M>;
         a.M = M;
         a.ps = L::PS;
         const size_t smem = L::bytes(a.in.nPhase * a.nAtom, a.nAtom);
         if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "z stage tables exceed shared memory");
-        QPD_TRY(set_smem(c, zstage_pipe<T, NZ, M, NT, RAD>, smem));
+        QPD_TRY(set_smem(c, zstage_pipe<T, NZ, M, NT, RAD, REGIN>, smem));
         int per_sm = 0, sms = 0;
-        QPD_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zstage_pipe<T, NZ, M, NT, RAD>, NT, smem));
+        QPD_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zstage_pipe<T, NZ, M, NT, RAD, REGIN>, NT,
+                                                                smem));
         QPD_CU(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
         const int64_t ntiles = (a.ncols + M - 1) / M;
         const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sms));
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
-        zstage_pipe<T, NZ, M, NT, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
+        zstage_pipe<T, NZ, M, NT, RAD, REGIN><<<(unsigned)grid, NT, smem, st>>>(a);
         return tstop(c, QPD_K_ZSTAGE, st, t0);
     }
 
@@ -630,8 +633,11 @@ template <typename T> struct Impl {
                 case 64: return smem_z_<64, F ? 16 : 8, F ? 512 : 256, Radix<8, 8>>(c, a, st);
                 case 68: return smem_z_<68, F ? 12 : 6, F ? 416 : 224, Pfa<4, 17>>(c, a, st);
                 case 104:
-                    if (F && c->knob_z == 1) return smem_z_<104, 8, 256, Pfa<8, 13>>(c, a, st);
-                    return smem_z_<104, F ? 8 : 4, F ? 416 : 224, Pfa<8, 13>>(c, a, st);
+                    // float: 256 threads with each thread's inputs in registers measured fastest (1.82 ms at
+                    // 512x512x104 against 1.86 for 416 threads reading them from shared memory per atom)
+                    if (F && c->knob_z == 1) return smem_z_<104, 8, 416, Pfa<8, 13>>(c, a, st);
+                    if (F) return smem_z_<104, 8, 256, Pfa<8, 13>, true>(c, a, st);
+                    return smem_z_<104, 4, 224, Pfa<8, 13>>(c, a, st);
                 case 128: return smem_z_<128, F ? 8 : 4, F ? 512 : 256, Radix<8, 4, 4>>(c, a, st);
             }
         }

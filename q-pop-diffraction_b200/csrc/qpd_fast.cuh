@@ -442,7 +442,7 @@ template <typename T, int NZ, int M> struct ZLayout {
     }
 };
 
-template <typename T, int NZ, int M, int NT, class RAD>
+template <typename T, int NZ, int M, int NT, class RAD, bool REGIN = false>
 __global__ void __launch_bounds__(NT, 2) zstage_pipe(ZArgs<T> a) {
     using C = C_t<T>;
     using L = ZLayout<T, NZ, M>;
@@ -562,22 +562,46 @@ __global__ void __launch_bounds__(NT, 2) zstage_pipe(ZArgs<T> a) {
         C accE[CPT], accX[CPT], accY[CPT];
 #pragma unroll
         for (int q = 0; q < CPT; q++) accE[q] = accX[q] = accY[q] = cmake<C>(0, 0);
+        // REGIN: each thread's cells' inputs stay in registers for all atoms
+        CellIn<T> rcl[REGIN ? CPT : 1];
+        int rph[REGIN ? CPT : 1];
+        T rwt[REGIN ? CPT : 1];
+        if constexpr (REGIN) {
+#pragma unroll
+            for (int q = 0; q < CPT; q++) {
+                const int e = tid + q * NT;
+                if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        rcl[q].p[k] = sin_[k * CELLS + e];
+                        rcl[q].u[k] = sin_[(3 + k) * CELLS + e];
+                    }
+                    rcl[q].tu = stu[e];
+                    rph[q] = single ? (int)sph[e] : -1;
+                    rwt[q] = single ? swt[e] : T(0);
+                }
+            }
+        }
 
         for (int at = 0; at < a.nAtom; at++) {
 #pragma unroll
             for (int q = 0; q < CPT; q++) {
                 const int e = tid + q * NT;
                 if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
-                    CellIn<T> cl;
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        cl.p[k] = sin_[k * CELLS + e];
-                        cl.u[k] = sin_[(3 + k) * CELLS + e];
-                    }
-                    cl.tu = stu[e];
                     C E, X, Y, Z;
-                    cell_source<T>(a.in, g0 + e, cl, single ? (int)sph[e] : -1, single ? swt[e] : T(0), apc,
-                                   a.nAtom, at, E, X, Y, Z);
+                    if constexpr (REGIN) {
+                        cell_source<T>(a.in, g0 + e, rcl[q], rph[q], rwt[q], apc, a.nAtom, at, E, X, Y, Z);
+                    } else {
+                        CellIn<T> cl;
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            cl.p[k] = sin_[k * CELLS + e];
+                            cl.u[k] = sin_[(3 + k) * CELLS + e];
+                        }
+                        cl.tu = stu[e];
+                        cell_source<T>(a.in, g0 + e, cl, single ? (int)sph[e] : -1, single ? swt[e] : T(0), apc,
+                                       a.nAtom, at, E, X, Y, Z);
+                    }
                     const int s = ssrc[q];
                     buf[s] = E;
                     buf[PLANE + s] = X;
