@@ -50,7 +50,7 @@ GRID = (512, 512, 104)
 REFLECTIONS = ((0, 0, 2), (1, 0, 3))
 METRIC = "Gcells/s per 3-D volume at 512x512x104 (float32 source+FFT, float64 phase reduction)"
 UNIT = "Gcells/s"
-CPU_SAMPLE = (128, 128, 104)        # cpu_baseline: about 10 s of NumPy work
+CPU_SAMPLE = (256, 384, 104)        # cpu_baseline: a bounded sample, several seconds of NumPy work
 REF_SAMPLE = (64, 64, 104)          # --impl reference: one step, so K + W steps end in minutes
 FALLBACK_HBM = 6650.0
 
@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None, help="steps of the host-buffer leg (default: min(K, 20))")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving (request loop) leg")
+    ap.add_argument("--serving-requests", type=int, default=400)
     return ap.parse_args()
 
 
@@ -193,6 +195,45 @@ def run_reference(args, rank):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+SERVING_SHAPES = ((128, 128, 128), (256, 256, 64), (512, 512, 104), (1024, 1024, 68))
+SERVING_HKLS = ((0, 0, 2), (1, 0, 3), (1, 1, 3), (2, 0, 0))
+
+
+def serving_leg(args, torch, device):
+    """
+    32 resident snapshots (8 per grid of the serving mix, vortex / twin / two-phase textures) and
+    Poisson requests over them and the 4 reflections.  Capacity: every request queued at once; then
+    an open-loop run at 80% of that rate.  Latency is arrival to completion, on the device.
+    """
+    from qpop_diffraction_b200 import workloads
+    from qpop_diffraction_b200.serving import Engine, Snapshot, SnapshotStore, latency_stats, poisson_requests
+    store = SnapshotStore()
+    for i in range(32):
+        shape = SERVING_SHAPES[i % 4]
+        kind = workloads.TEXTURES[(i // 4) % 3]
+        params, inputs = workloads.gpu_snapshot(kind, shape, seed=1000 + i, device=f"cuda:{device}")
+        store.add(Snapshot(i, kind, shape, params, inputs))
+    free, total = torch.cuda.mem_get_info(device)
+    budget = int(min(free - (8 << 30), 64 << 30))
+    eng = Engine(store, budget, device=device)
+    try:
+        for i in range(4):                      # two slots per grid where the budget allows
+            eng.reserve(i, 2)
+        eng.warm([(i, h) for i in range(32) for h in SERVING_HKLS])
+        ids = list(range(32))
+        cap = latency_stats(eng.run(poisson_requests(args.serving_requests, 0, ids, SERVING_HKLS, seed=1)))
+        rate = 0.8 * cap["volumes_per_s"]
+        load = latency_stats(eng.run(poisson_requests(args.serving_requests, rate, ids, SERVING_HKLS, seed=2)))
+        out = {"grids": [list(s) for s in SERVING_SHAPES], "snapshots": 32, "reflections": [list(h) for h in SERVING_HKLS],
+               "capacity_volumes_per_s": cap["volumes_per_s"], "offered_rate_per_s": rate, "p50_ms": load["p50_ms"],
+               "p99_ms": load["p99_ms"], "volumes_per_s": load["volumes_per_s"], "requests": load["requests"],
+               "slots": eng.peak_slots, "hbm_budget_gb": budget / 1e9, "resident_snapshots_gb": store.nbytes / 1e9,
+               "latency": "arrival to completion on the device, open-loop Poisson arrivals at 80% of capacity"}
+    finally:
+        eng.close()
+    return out
 
 
 def main():
@@ -337,6 +378,13 @@ def main():
         for v in fp64.values():
             v["fp32_speedup"] = v["ms_per_step"] / (ms / args.steps)
 
+    # ---------------- serving: Poisson mix of grids over resident snapshots ----------------
+    serving = None
+    if not args.no_serving:
+        del d64
+        torch.cuda.empty_cache()
+        serving = serving_leg(args, torch, local)
+
     # ---------------- CPU baseline ----------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -359,7 +407,7 @@ def main():
                        "l2": "no flush: every step reads and writes about 4 GB, far above the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "roofline": roof, "model_roofline": model, "kernels": per_kernel, "gpu_launches": launches,
-            "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "e2e": e2e, "fp64": fp64, "serving": serving, "cpu_baseline": cpu, "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

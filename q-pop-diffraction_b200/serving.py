@@ -1,0 +1,249 @@
+"""
+Continuous-batching request loop for diffraction volumes on one GPU.
+
+Requests name a resident snapshot and a reflection hkl.  The engine:
+
+* keeps every snapshot's packed inputs resident in HBM (``SnapshotStore``);
+* runs each volume in a *slot*: a planned context for one grid shape with its own workspace,
+  output buffer and CUDA stream.  Slots are created on demand while their HBM footprint fits the
+  engine's budget (admission by footprint); a request whose shape has no free slot and no room
+  for a new one waits;
+* dispatches a waiting request as soon as a slot of its shape is free, so requests that arrive
+  while others run start at once and their kernels overlap with the running ones on other
+  streams (continuous batching, not a FIFO queue: a request of a free shape overtakes one whose
+  shape is busy);
+* replays a CUDA graph per (slot, snapshot, reflection), captured on first use, so a dispatch
+  is one table upload and one graph launch.
+
+Latency is measured from a request's arrival to the moment the host sees its completion event.
+"""
+
+from __future__ import annotations
+
+import collections
+import dataclasses
+import time
+
+import numpy as np
+
+from .plan import Plan, crystal_from
+
+
+@dataclasses.dataclass
+class Snapshot:
+    id: int
+    kind: str
+    shape: tuple
+    params: object
+    inputs: dict
+
+    @property
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in self.inputs.values() if t is not None)
+
+
+class SnapshotStore:
+    """Resident packed snapshots, keyed by id."""
+
+    def __init__(self):
+        self.snaps = {}
+
+    def add(self, snap: Snapshot):
+        self.snaps[snap.id] = snap
+        return snap
+
+    def __getitem__(self, i):
+        return self.snaps[i]
+
+    def __len__(self):
+        return len(self.snaps)
+
+    @property
+    def nbytes(self):
+        return sum(s.nbytes for s in self.snaps.values())
+
+
+@dataclasses.dataclass
+class Request:
+    id: int
+    snapshot: int
+    hkl: tuple
+    arrival: float = 0.0      # seconds from the start of the run
+    start: float = None       # dispatch time
+    done: float = None        # completion seen by the host
+    slot: object = None
+
+    @property
+    def latency(self):
+        return None if self.done is None else self.done - self.arrival
+
+
+class Slot:
+    """One in-flight volume's worth of resources for a grid shape."""
+
+    def __init__(self, shape, spacing, nPhase, device, crystal_of):
+        import torch
+        self.shape, self.spacing = tuple(shape), tuple(spacing)
+        self.plan = Plan(shape, spacing, nPhase, 3, precision="fp32", device=device)
+        self.device = torch.device("cuda", device)
+        self.stream = torch.cuda.Stream(self.device)
+        self.out = torch.empty(self.shape, dtype=torch.float64, device=self.device)
+        self.event = torch.cuda.Event()
+        self.graphs = {}
+        self.crystal_of = crystal_of
+        self.request = None
+        self.warm = False
+        # the workspace exists once a crystal is set: plan one now so the footprint is known
+        self.plan.set_crystal(crystal_of((0, 0, 2)))
+        self.footprint = self.plan.workspace_bytes + self.out.numel() * 8
+
+    def launch(self, snap: Snapshot, hkl):
+        import torch
+        self.plan.set_crystal(self.crystal_of(hkl))
+        key = (snap.id, tuple(hkl))
+        g = self.graphs.get(key)
+        if g is None:
+            if not self.warm:
+                # one direct run sets the kernels' launch attributes before any capture
+                self.plan.run_device(snap.inputs, self.out, stream=self.stream.cuda_stream)
+                self.stream.synchronize()
+                self.warm = True
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=self.stream, capture_error_mode="relaxed"):
+                self.plan.run_device(snap.inputs, self.out, stream=self.stream.cuda_stream)
+            self.graphs[key] = g
+        with torch.cuda.stream(self.stream):
+            g.replay()
+            self.event.record(self.stream)
+
+    def close(self):
+        self.graphs.clear()
+        self.plan.close()
+
+
+class Engine:
+    """Admission by HBM footprint, per-shape slots, continuous dispatch."""
+
+    def __init__(self, store: SnapshotStore, hbm_budget_bytes, device=0, crystal_of=None):
+        from . import workloads
+        self.store = store
+        self.budget = int(hbm_budget_bytes)
+        self.device = device
+        self.crystal_of = crystal_of or (lambda params, hkl: crystal_from(params, workloads.serving_crystal(hkl)))
+        self.slots = collections.defaultdict(list)   # shape -> [Slot]
+        self.used = 0
+        self.peak_slots = 0
+
+    def _free_slot(self, snap):
+        for s in self.slots[snap.shape]:
+            if s.request is None:
+                return s
+        return self._new_slot(snap)
+
+    def _new_slot(self, snap):
+        """A new slot for the snapshot's shape, if its footprint fits the budget."""
+        params = snap.params
+        probe_bytes = self._footprint_estimate(snap)
+        if self.used + probe_bytes > self.budget:
+            return None
+        s = Slot(snap.shape, (params.dx, params.dy, params.dz), params.nPhase, self.device,
+                 lambda hkl, p=params: self.crystal_of(p, hkl))
+        self.used += s.footprint
+        self.slots[snap.shape].append(s)
+        self.peak_slots = max(self.peak_slots, sum(len(v) for v in self.slots.values()))
+        return s
+
+    @staticmethod
+    def _footprint_estimate(snap):
+        # fields of the fused schedule (3 per (R_x, R_y) group of the 5-atom cell: 12 complex64) + float64 I + tables
+        n = int(np.prod(snap.shape))
+        return n * (12 * 8 + 8) + (1 << 22)
+
+    def dispatch(self, req: Request, now):
+        snap = self.store[req.snapshot]
+        slot = self._free_slot(snap)
+        if slot is None:
+            return False
+        slot.request = req
+        req.slot = slot
+        req.start = now
+        slot.launch(snap, req.hkl)
+        return True
+
+    def poll(self, now, finished):
+        for slots in self.slots.values():
+            for s in slots:
+                if s.request is not None and s.event.query():
+                    s.request.done = now
+                    finished.append(s.request)
+                    s.request = None
+
+    def busy(self):
+        return any(s.request is not None for v in self.slots.values() for s in v)
+
+    def reserve(self, snap_id, count):
+        """Create up to `count` slots for a snapshot's shape, as far as the budget allows."""
+        snap = self.store[snap_id]
+        while len(self.slots[snap.shape]) < count and self._new_slot(snap) is not None:
+            pass
+        return len(self.slots[snap.shape])
+
+    def warm(self, pairs):
+        """Capture, on every slot of its shape, the graph of each (snapshot, hkl) pair ahead of a timed run."""
+        for snap_id, hkl in pairs:
+            snap = self.store[snap_id]
+            for s in self.slots[snap.shape]:
+                s.launch(snap, hkl)
+                s.stream.synchronize()
+
+    def run(self, requests, result_of=None):
+        """
+        Serve requests (arrival times in seconds from now, sorted).  Returns them with start and done
+        times set.  result_of(request, tensor) is called on completion with the slot's output.
+        """
+        waiting = collections.deque()
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        finished = []
+        t0 = time.perf_counter()
+        while pending or waiting or self.busy():
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(pending.popleft())
+            # dispatch every waiting request that has a free slot (later ones may overtake a blocked head)
+            for _ in range(len(waiting)):
+                r = waiting.popleft()
+                if not self.dispatch(r, time.perf_counter() - t0):
+                    waiting.append(r)
+            done_before = len(finished)
+            self.poll(time.perf_counter() - t0, finished)
+            if result_of is not None:
+                for r in finished[done_before:]:
+                    r.slot.stream.synchronize()
+                    result_of(r, r.slot.out)
+            if not (waiting or pending) and not self.busy():
+                break
+            time.sleep(0)
+        return finished
+
+    def close(self):
+        for v in self.slots.values():
+            for s in v:
+                s.close()
+        self.slots.clear()
+        self.used = 0
+
+
+def poisson_requests(n, rate, snapshots, hkls, seed=0):
+    """n requests with exponential inter-arrival times (rate per second), uniform over snapshots and hkls."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n)) if rate > 0 else np.zeros(n)
+    snaps = rng.integers(0, len(snapshots), size=n)
+    hk = rng.integers(0, len(hkls), size=n)
+    return [Request(i, int(snapshots[snaps[i]]), tuple(hkls[hk[i]]), float(t[i])) for i in range(n)]
+
+
+def latency_stats(finished):
+    lat = np.array([r.latency for r in finished])
+    span = max(r.done for r in finished) - min(r.arrival for r in finished)
+    return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3), "volumes_per_s": len(finished) / span, "requests": len(finished)}

@@ -236,3 +236,89 @@ def random_case(shape, seed, nPhase=1, weights="onehot", hkl=(1, 0, 3), strain=F
             region = region * rng.uniform(0.2, 1.0, size=n)
     return Case(f"random_{'x'.join(map(str, shape))}_{weights}", params, atoms, f32(oPhase).ravel(), f32(P).ravel(),
                 f32(U).ravel(), f32(region), seed)
+
+
+# ---------------------------------------------------------------------------------------------
+# Snapshots generated on the GPU, directly in the packed layout the kernels read (float32 P and
+# u planes, int8 phase index): the serving mix and the 4000 x 4000 x 68 grid are too large to
+# build in NumPy float64 in reasonable time.  Seeded with torch.Generator on the device.
+# ---------------------------------------------------------------------------------------------
+
+TEXTURES = ("vortex", "twin", "twophase")
+
+
+def gpu_snapshot(kind, shape, seed, device="cuda", substrate=None, n_domains=200, spacing=(0.39, 0.39, 0.40)):
+    """
+    Packed inputs of a seeded film snapshot on the GPU.  Two phases: substrate (phase 0) for
+    z < substrate (default a quarter of the box, at most 24 cells), film (phase 1) above.
+
+    kind "vortex":   polar-vortex array rotating in x-z, period 10 cells, |P| = 0.6, plus N(0, 0.02);
+                     u = 1% strain gradient up z + small modes (config 2 texture).
+    kind "twin":     in-plane Voronoi tessellation of n_domains cells, 3 variants with P along
+                     directions 120 degrees apart starting at [110], |P| = 0.5; u_z from a
+                     +-0.5% strain per domain (config 3 texture).
+    kind "twophase": a1/a2 stripes with period 16 along [110], |P| = 0.5, on the strained substrate.
+    Returns (params, inputs) with inputs = {"P", "U", "phase", "weight": None, "wdense": None}.
+    """
+    import torch
+
+    nx, ny, nz = (int(s) for s in shape)
+    n = nx * ny * nz
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed))
+    params = make_params(shape, spacing, 2)
+    if substrate is None:
+        substrate = min(24, nz // 4)
+    f32 = dict(dtype=torch.float32, device=dev)
+    x = torch.arange(nx, **f32).view(nx, 1, 1)
+    y = torch.arange(ny, **f32).view(1, ny, 1)
+    z = torch.arange(nz, **f32).view(1, 1, nz)
+    film = (z >= substrate).expand(nx, ny, nz)
+    P = torch.empty((3, nx, ny, nz), **f32)
+    P.normal_(0.0, 0.02, generator=g)
+    if kind == "vortex":
+        k = 2 * math.pi / 10
+        dz_psi = torch.sin(k * x) * torch.cos(k * z)
+        dx_psi = torch.cos(k * x) * torch.sin(k * z)
+        norm = torch.clamp(torch.sqrt(dz_psi ** 2 + dx_psi ** 2), min=1e-12)
+        P[0] += torch.where(film, (0.6 * dz_psi / norm).expand(nx, ny, nz), 0.0)
+        P[2] += torch.where(film, (-0.6 * dx_psi / norm).expand(nx, ny, nz), 0.0)
+        strain = 0.01 * z / max(nz - 1, 1)
+    elif kind == "twin":
+        seeds = torch.rand((n_domains, 2), generator=g, **f32) * torch.tensor([nx, ny], **f32)
+        variant = torch.randint(0, 3, (n_domains,), generator=g, device=dev)
+        dstrain = (torch.rand(n_domains, generator=g, **f32) * 2 - 1) * 0.005
+        # nearest seed per (x, y) column, in row blocks to bound the temporary
+        owner = torch.empty((nx, ny), dtype=torch.long, device=dev)
+        xs = torch.arange(nx, **f32)
+        ys = torch.arange(ny, **f32)
+        step = max(1, (1 << 24) // max(1, ny * n_domains))
+        for i0 in range(0, nx, step):
+            dx = xs[i0:i0 + step].view(-1, 1, 1) - seeds[:, 0].view(1, 1, -1)
+            dy = ys.view(1, -1, 1) - seeds[:, 1].view(1, 1, -1)
+            owner[i0:i0 + step] = torch.argmin(dx * dx + dy * dy, dim=2)
+        ang = math.pi / 4 + variant[owner].to(torch.float32) * (2 * math.pi / 3)
+        filmf = film.to(torch.float32)
+        P[0] += (0.5 * torch.cos(ang)).unsqueeze(2) * filmf
+        P[1] += (0.5 * torch.sin(ang)).unsqueeze(2) * filmf
+        strain = dstrain[owner].unsqueeze(2).expand(nx, ny, nz)
+    elif kind == "twophase":
+        a1 = (((x + y) % 16) < 8).expand(nx, ny, nz)
+        P[0] += torch.where(film & a1, 0.5, 0.0)
+        P[1] += torch.where(film & ~a1, 0.5, 0.0)
+        strain = 0.004 * (z < substrate).to(torch.float32)
+    else:
+        raise ValueError(f"unknown texture {kind!r}")
+    strain = torch.as_tensor(strain, **f32).expand(nx, ny, nz)
+    uz = (torch.cumsum(strain, dim=2) - 0.5 * strain) * params.dz
+    U = torch.empty((3, nx, ny, nz), **f32)
+    U.normal_(0.0, 0.001, generator=g)
+    U[2] += uz
+    phase = film.to(torch.int8).contiguous().view(-1)
+    return params, {"P": P.view(-1), "U": U.view(-1), "phase": phase, "weight": None, "wdense": None}
+
+
+def serving_crystal(hkl, seed=2):
+    """The two-phase perovskite crystal of the serving mix at reflection hkl (config-2 constants)."""
+    return config2_crystal(seed, hkl)
