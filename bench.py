@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving (request loop) leg")
     ap.add_argument("--serving-requests", type=int, default=400)
+    ap.add_argument("--config", type=int, default=2, choices=(2, 3),
+                    help="3: the 4000x4000x68 twin film on one GPU (device-resident, per-pass roofline)")
+    ap.add_argument("--validate", action="store_true", help="with --config 3: compare against a float64 plain run")
     return ap.parse_args()
 
 
@@ -197,6 +200,87 @@ def run_reference(args, rank):
     }), flush=True)
 
 
+CONFIG3 = (4000, 4000, 68)
+
+
+def run_config3(args, torch, dev, rank, world):
+    """
+    The 4000 x 4000 x 68 three-variant Voronoi twin film (1.09e9 cells, one phase, G = 113) on one
+    GPU: generated on the device, float32 fused schedule, inputs resident.  With --validate, the
+    same volume in float64 with the plain (per atom and component) schedule, compared on the GPU.
+    """
+    from qpop_diffraction_b200 import Plan, crystal_from, replicas, workloads
+    shape = tuple(args.grid) if tuple(args.grid) != GRID else CONFIG3
+    params, inputs = workloads.gpu_snapshot("twin", shape, seed=3 + rank, device=dev, n_phase=1)
+    crystal = crystal_from(params, workloads.config3_crystal(3, (1, 1, 3)))
+    n = params.n
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    plan = Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp32", device=dev.index)
+    plan.set_crystal(crystal)
+    out = torch.empty(shape, dtype=torch.float64, device=dev)
+    for _ in range(args.warmup):
+        plan.run_device(inputs, out)
+    torch.cuda.synchronize(dev)
+    plan.device_status()
+    plan.stage_times()
+    plan.enable_timing(True)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.run_device(inputs, out)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    plan.device_status()
+    ms = replicas.slowest(e0.elapsed_time(e1), dev) / args.steps
+    stage = plan.stage_times()
+    hbm, hbm_src = peaks()
+    g1, g2 = atom_groups(crystal.R)
+    kb = kernel_bytes(n, g1, g2, False)
+    kernels = {k: {"avg_ms": t / c, "bytes_per_launch": kb[k], "gbs": kb[k] / (t / c * 1e-3) / 1e9,
+                   "frac": kb[k] / (t / c * 1e-3) / 1e9 / hbm} for k, (t, c) in stage.items() if k in kb}
+    line = {"metric": f"Gcells/s per 3-D volume at {'x'.join(map(str, shape))} (float32, one GPU)",
+            "value": replicas.throughput(n, ms * 1e-3, world) / 1e9, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "dtype": "f32", "data": "synthetic (seeded Voronoi twin film, generated on the GPU)",
+            "config": {"workload": f"three-variant Voronoi twin film {'x'.join(map(str, shape))}, 200 domains, "
+                                   f"5 atoms, 1 phase, G=113", "cells": n},
+            "kernels": kernels, "peak_gbs": hbm, "peak_source": f"hbm_gbs of {hbm_src}",
+            "device_memory_peak_gb": (torch.cuda.max_memory_allocated(dev) + plan.workspace_bytes) / 1e9}
+    if args.validate:
+        I32 = out
+        plan.close()
+        del plan
+        torch.cuda.empty_cache()
+        in64 = {"P": inputs["P"].double(), "U": inputs["U"].double(), "phase": inputs["phase"], "weight": None,
+                "wdense": None}
+        del inputs
+        torch.cuda.empty_cache()
+        p64 = Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp64", schedule="plain",
+                   device=dev.index)
+        p64.set_crystal(crystal)
+        I64 = torch.empty(shape, dtype=torch.float64, device=dev)
+        t = time.perf_counter()
+        p64.run_device(in64, I64)
+        torch.cuda.synchronize(dev)
+        p64.device_status()
+        t64 = time.perf_counter() - t
+        imax = I64.max()
+        strong = I64 > 1e-6 * imax
+        line["validation"] = {
+            "against": "float64 plain schedule of the same kernels on the full grid",
+            "max_abs_dI_over_Imax": float((I32 - I64).abs().max() / imax),
+            "max_rel_err_above_1e-6_Imax": float(((I32 - I64).abs()[strong] / I64[strong]).max()),
+            "max_abs_dlog10I_above_1e-6_Imax": float((torch.log10(I32[strong]) - torch.log10(I64[strong])).abs().max()),
+            "fp64_plain_seconds": t64}
+        p64.close()
+    else:
+        plan.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 SERVING_SHAPES = ((128, 128, 128), (256, 256, 64), (512, 512, 104), (1024, 1024, 68))
 SERVING_HKLS = ((0, 0, 2), (1, 0, 3), (1, 1, 3), (2, 0, 0))
 
@@ -250,6 +334,9 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.config == 3:
+        run_config3(args, torch, dev, rank, world)
+        return
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)

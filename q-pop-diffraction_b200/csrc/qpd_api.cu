@@ -673,7 +673,7 @@ template <typename T> struct Impl {
 
     template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF>
     static int tma_axis_b(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
-        constexpr int BOX = N > 256 ? 256 : N;
+        constexpr int BOX = tma_rows(N, CZ * (int)sizeof(C));
         a.Cz = CZ;
         a.nzc = (a.nz + CZ - 1) / CZ;
         CUtensorMap map;
@@ -724,6 +724,17 @@ template <typename T> struct Impl {
             case 256: return fast_axis_n<256, 256, EPI, Radix<8, 8, 4>>(c, a, nouter, kind, st);
             case 512: return fast_axis_n<512, 512, EPI, Radix<8, 8, 8>>(c, a, nouter, kind, st);
             case 1024: return fast_axis_n<1024, 1024, EPI, Radix<8, 8, 4, 4>>(c, a, nouter, kind, st);
+            case 4000:
+                // 4000 x 2 tiles (16-byte rows: the other half of each 32-byte sector is read by the CTA of
+                // the neighbouring z chunk while it is still in L2), 200-row boxes, two buffers
+                if constexpr (sizeof(T) == 4) {
+                    if (c->tma && a.nz % 2 == 0) {
+                        const bool xp = kind == QPD_K_XPASS || (kind == QPD_K_AXIS && a.stride != a.nz);
+                        if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, Radix<8, 4, 5, 5, 5>, 2>(c, a, nouter, kind, st);
+                        return tma_axis_b<4000, 2, 512, 2, EPI, false, Radix<8, 4, 5, 5, 5>, 2>(c, a, nouter, kind, st);
+                    }
+                }
+                break;
         }
         *done = false;
         return QPD_OK;
@@ -1033,7 +1044,9 @@ int check_status(qpd_ctx* c) {
     QPD_CU(c, cudaMemcpy(&v, c->status.p, sizeof v, cudaMemcpyDeviceToHost));
     if (v == 0) return QPD_OK;
     QPD_CU(c, cudaMemset(c->status.p, 0, sizeof v));
-    return fail(c, QPD_ERR_CUDA, "a kernel gave up waiting for its tile loads (device status %d)", v);
+    return fail(c, QPD_ERR_CUDA, "device status %d: %s", v,
+                v == QPD_DEVERR_ALIGN ? "shared memory was not aligned for TMA, the kernel stopped before loading"
+                                      : "a kernel gave up waiting for its tile loads");
 }
 
 int use_device(qpd_ctx* c) {

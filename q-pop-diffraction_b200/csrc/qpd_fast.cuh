@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(NT) zstage_fast(ZArgs<T> a) {
     constexpr int CELLS = M * NZ;
     constexpr int CPT = cdiv(CELLS, NT);
     using GE = Geo<4 * M, 4 * M, PS, 0, 1, NT>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* buf = reinterpret_cast<C*>(smem_raw);
     AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(buf + 4 * PLANE);
     const int tid = threadIdx.x;
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
     constexpr int EP = cdiv(GROUPS, NT);          // slots per thread
     constexpr int CV = CZ / VEC;                  // slots per row
     using GE = Geo<CZ, CZ, 1, 0, CZ, NT>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* buf = reinterpret_cast<C*>(smem_raw);
     const int tid = threadIdx.x;
     const long long outer = blockIdx.x / a.nzc;
@@ -250,8 +250,17 @@ __global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
 // (2 nz reals, ny, nfields * nx); XPASS selects rows along x (box 2CZ x 1 x BOX) instead of
 // along y (box 2CZ x BOX x 1).  Out-of-range z of a partial chunk arrives as zeros.
 // ---------------------------------------------------------------------------------------
+// Rows per TMA box: the largest divisor of N that is at most 256 (a box dimension's limit) and whose
+// box of `row_bytes`-byte rows is a multiple of 128 bytes, since every box lands at a 128-byte
+// aligned shared-memory address.  0 when no such divisor exists.
+__host__ __device__ constexpr int tma_rows(int N, int row_bytes) {
+    for (int b = N < 256 ? N : 256; b > 0; b--)
+        if (N % b == 0 && (b * row_bytes) % 128 == 0) return b;
+    return 0;
+}
+
 template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF>
-__global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
+__global__ void __launch_bounds__(NT, NT <= 512 && N * CZ * NBUF <= 8192 ? 2 : 1) axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
     using C = C_t<T>;
     static_assert(CZ % VEC == 0, "chunk must hold whole vectors");
     constexpr int NO = 1;  // the host builds single-output segments for this kernel
@@ -259,8 +268,9 @@ __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) axis_tma(const __grid_c
     constexpr int GROUPS = TILE / VEC;
     constexpr int EP = cdiv(GROUPS, NT);
     constexpr int CV = CZ / VEC;
-    constexpr int BOX = N > 256 ? 256 : N;
-    static_assert(N % BOX == 0, "rows must split into whole boxes");
+    constexpr int BOX = tma_rows(N, CZ * (int)sizeof(C));
+    static_assert(BOX > 0 && N % BOX == 0, "rows must split into whole boxes of 128-byte multiples");
+    static_assert((TILE * sizeof(C)) % 128 == 0, "tile buffers must start 128-byte aligned");
     constexpr uint32_t BYTES = TILE * sizeof(C);
     using GE = Geo<CZ, CZ, 1, 0, CZ, NT>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -298,6 +308,10 @@ __global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) axis_tma(const __grid_c
         }
     };
 
+    if (smem_u32(smem_raw) % 128 != 0) {  // TMA destinations must be 128-byte aligned: refuse, do not load
+        if (tid == 0) atomicExch(a.status, QPD_DEVERR_ALIGN);
+        return;
+    }
     if (tid == 0) {
         for (int b = 0; b < NBUF; b++) mbar_init(&bar[b], 1);
         fence_barrier_init();
@@ -467,6 +481,10 @@ __global__ void __launch_bounds__(NT, 2) zstage_pipe(ZArgs<T> a) {
         scu[i] = a.coefUz[i];
     }
 
+    if (smem_u32(smem_raw) % 16 != 0) {  // bulk-copy destinations must be 16-byte aligned: refuse, do not load
+        if (tid == 0) atomicExch(a.status, QPD_DEVERR_ALIGN);
+        return;
+    }
     const bool single = a.in.wdense == nullptr;
     const long long ntiles = (a.ncols + M - 1) / M;
     const bool aligned = (a.in.n * sizeof(T)) % 16 == 0 && a.in.nStruc == 3 &&

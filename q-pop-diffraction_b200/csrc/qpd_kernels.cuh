@@ -185,7 +185,7 @@ template <typename T> struct ZArgs {
 template <typename T, int NT, int EPT>
 __global__ void __launch_bounds__(NT) zstage_kernel(ZArgs<T> a) {
     using C = C_t<T>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* buf = reinterpret_cast<C*>(smem_raw);
     const int plane = a.M * a.ps;
     AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(buf + 4 * plane);
@@ -308,7 +308,7 @@ template <typename T> struct AxisArgs {
 template <typename T, int NT, int EPT, bool EPI>
 __global__ void __launch_bounds__(NT) axis_kernel(AxisArgs<T> a) {
     using C = C_t<T>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* buf = reinterpret_cast<C*>(smem_raw);
     const int tid = threadIdx.x;
     const long long outer = blockIdx.x / a.nzc;
@@ -438,7 +438,7 @@ template <typename T> struct FftzArgs {
 template <typename T, int NT, int EPT>
 __global__ void __launch_bounds__(NT) fftz_kernel(FftzArgs<T> a) {
     using C = C_t<T>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* sb = reinterpret_cast<C*>(smem_raw);
     const int tid = threadIdx.x;
     const long long c0 = (long long)blockIdx.x * a.M;

@@ -14,6 +14,7 @@ namespace qpd {
 
 constexpr long long kWaitLimit = 1LL << 24;  // try_wait polls (each may suspend briefly): seconds, not forever
 constexpr int QPD_DEVERR_TIMEOUT = 1;
+constexpr int QPD_DEVERR_ALIGN = 2;  // dynamic shared memory not 128-byte aligned: no TMA load was issued
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 

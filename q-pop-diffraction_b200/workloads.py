@@ -247,7 +247,8 @@ def random_case(shape, seed, nPhase=1, weights="onehot", hkl=(1, 0, 3), strain=F
 TEXTURES = ("vortex", "twin", "twophase")
 
 
-def gpu_snapshot(kind, shape, seed, device="cuda", substrate=None, n_domains=200, spacing=(0.39, 0.39, 0.40)):
+def gpu_snapshot(kind, shape, seed, device="cuda", substrate=None, n_domains=200, spacing=(0.39, 0.39, 0.40),
+                 n_phase=2):
     """
     Packed inputs of a seeded film snapshot on the GPU.  Two phases: substrate (phase 0) for
     z < substrate (default a quarter of the box, at most 24 cells), film (phase 1) above.
@@ -258,6 +259,7 @@ def gpu_snapshot(kind, shape, seed, device="cuda", substrate=None, n_domains=200
                      directions 120 degrees apart starting at [110], |P| = 0.5; u_z from a
                      +-0.5% strain per domain (config 3 texture).
     kind "twophase": a1/a2 stripes with period 16 along [110], |P| = 0.5, on the strained substrate.
+    n_phase=1: one phase everywhere (no substrate), as in the 4000 x 4000 x 68 twin film.
     Returns (params, inputs) with inputs = {"P", "U", "phase", "weight": None, "wdense": None}.
     """
     import torch
@@ -267,8 +269,10 @@ def gpu_snapshot(kind, shape, seed, device="cuda", substrate=None, n_domains=200
     dev = torch.device(device)
     g = torch.Generator(device=dev)
     g.manual_seed(int(seed))
-    params = make_params(shape, spacing, 2)
-    if substrate is None:
+    params = make_params(shape, spacing, n_phase)
+    if n_phase == 1:
+        substrate = 0
+    elif substrate is None:
         substrate = min(24, nz // 4)
     f32 = dict(dtype=torch.float32, device=dev)
     x = torch.arange(nx, **f32).view(nx, 1, 1)
@@ -315,8 +319,22 @@ def gpu_snapshot(kind, shape, seed, device="cuda", substrate=None, n_domains=200
     U = torch.empty((3, nx, ny, nz), **f32)
     U.normal_(0.0, 0.001, generator=g)
     U[2] += uz
-    phase = film.to(torch.int8).contiguous().view(-1)
+    if n_phase == 1:
+        phase = torch.zeros(n, dtype=torch.int8, device=dev)
+    else:
+        phase = film.to(torch.int8).contiguous().view(-1)
     return params, {"P": P.view(-1), "U": U.view(-1), "phase": phase, "weight": None, "wdense": None}
+
+
+def config3_crystal(seed=3, hkl=(1, 1, 3)):
+    """One-phase perovskite of the 4000 x 4000 x 68 twin film: aC = diag(0.39, 0.39, 0.40) nm,
+    Cromer-Mann form factors at |G|, ionic shifts k P with k in U[-0.02, 0.05] nm per C/m^2."""
+    rng = np.random.default_rng([seed] + list(hkl))
+    aC = np.diag([0.39, 0.39, 0.40])
+    q00 = q00_for(aC, hkl)
+    nAtom = len(PEROVSKITE)
+    fAtom = cromer_mann(rng, np.linalg.norm(q00), (1, nAtom))
+    return make_atoms(aC, q00, PEROVSKITE, fAtom, isotropic_shifts(rng.uniform(-0.02, 0.05, size=(1, nAtom))))
 
 
 def serving_crystal(hkl, seed=2):
