@@ -22,8 +22,35 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libqpopdiff.so")
 
 
+EXAMPLE = "polar_vortex_example"
+
+
 def golden_names():
-    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+    """Fixtures of seeded synthetic inputs (the FerroDyn example has its own loader)."""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem != EXAMPLE)
+
+
+def load_example():
+    """
+    The reference's disordered polar-vortex example (tests/golden/make_legacy_case.py) as FerroDyn
+    fields in file order (nz, ny, nx), the per-material tables, the grid and crystal, and the
+    reference's own diffraction() result.
+    """
+    from qpop_diffraction_b200 import workloads
+
+    z = np.load(GOLDEN / f"{EXAMPLE}.npz", allow_pickle=False)
+    shape = tuple(int(s) for s in z["shape"])
+    fe = [int(m) for m in z["fe_ids"]]
+    return SimpleNamespace(
+        shape=shape,
+        params=workloads.make_params(shape, z["spacing"], int(z["nPhase"]), z["strainAvg"], int(z["nStruc"])),
+        atoms=workloads.make_atoms(z["aC"], z["q00"], z["xAtom"], z["fAtom"], z["su"]),
+        P=np.ascontiguousarray(z["P"].transpose(0, 3, 2, 1)),
+        mat=np.ascontiguousarray(z["mat"].transpose(2, 1, 0)),
+        region=np.ascontiguousarray(z["region"].reshape(shape).transpose(2, 1, 0)),
+        dc=z["dc"], ramp_dz=float(z["ramp_dz"]),
+        phase_of=np.array([fe.index(m) if m in fe else -1 for m in range(len(z["dc"]))], dtype=np.int32),
+        uz_ref=z["uz_ref"], I=z["I"], qx=z["qx"], qy=z["qy"], qz=z["qz"])
 
 
 def load_golden(name):

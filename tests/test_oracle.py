@@ -74,3 +74,50 @@ def test_planted_oracle_fails_on_a_planted_mistake():
         return oracle.diffraction(params, atoms2, oPhase, oStruc, u, region)
     with pytest.raises(AssertionError):
         analytic.check_structure_factor(wrong, "c+", (0, 0, 2))
+
+
+# ---------------- the FerroDyn example and the boundary-input preparation ----------------
+
+def test_oracle_matches_reference_on_the_ferrodyn_example():
+    """The disordered polar-vortex example, prepared as the CLI does, against the reference's own run."""
+    from conftest import load_example
+    from oracle import fields_oracle
+    ex = load_example()
+    oPhase, oStruc, u, region = fields_oracle.prepare(ex.P, ex.mat, ex.dc, ex.phase_of, ex.ramp_dz, region=ex.region)
+    assert np.array_equal(u[2 * (u.size // 3):], ex.uz_ref)
+    I, qx, qy, qz = oracle.diffraction(ex.params, ex.atoms, oPhase, oStruc, u, region)
+    for got, want in zip((qx, qy, qz), (ex.qx, ex.qy, ex.qz)):
+        assert np.array_equal(got, want)
+    np.testing.assert_allclose(I, ex.I, rtol=1e-12, atol=1e-13 * ex.I.max())
+
+
+def test_fields_oracle_restates_the_cli_prep():
+    """prepare() against a literal transcription of src/python/cli.py:187-217 on a cropped two-material stack."""
+    from oracle import fields_oracle
+    rng = np.random.default_rng(5)
+    nxf, nyf, nzf = 6, 5, 20
+    lims = (1, 4), (0, 3), (3, 14)
+    sl = tuple(slice(a, b + 1) for a, b in lims)
+    mat_xyz = np.where(np.arange(nzf)[None, None, :] < 8, 0, 2) * np.ones((nxf, nyf, 1), dtype=int)
+    mat_xyz[rng.random(mat_xyz.shape) < 0.1] = 1                       # air pockets: not FE
+    fe_ids, dc_table, dz = [0, 2], np.array([-0.011, 0.0, 0.024]), 0.4
+    P_xyz = rng.standard_normal((3, nxf, nyf, nzf)).astype(np.float32)
+    u_xyz = (rng.standard_normal((3, nxf, nyf, nzf)) * 1e-11).astype(np.float32)
+    reg_xyz = rng.random((nxf, nyf, nzf)).astype(np.float32)
+    # the reference's arithmetic, step by step
+    oPhase = np.stack([mat_xyz[sl] == m for m in fe_ids]).astype(np.float64)
+    region = oPhase.sum(axis=0).ravel() * reg_xyz[sl].astype(np.float64).ravel()
+    dc = dc_table[mat_xyz]
+    uz_ref = ((np.cumsum(dc, axis=2) - 0.5 * dc) * dz)[sl].ravel()
+    u = np.stack([c[sl] for c in u_xyz]).astype(np.float64).ravel() / 1e-9
+    n = region.size
+    u[2 * n:] += uz_ref
+    oStruc = np.stack([c[sl] for c in P_xyz]).astype(np.float64).ravel()
+    # the oracle, from file-order arrays
+    f = lambda a: np.ascontiguousarray(a.transpose(*range(a.ndim - 3), a.ndim - 1, a.ndim - 2, a.ndim - 3))
+    cut = (sl[2], sl[1], sl[0])
+    got = fields_oracle.prepare(f(P_xyz)[(slice(None),) + cut], f(mat_xyz[sl[0], sl[1], :]), dc_table, [0, -1, 1], dz,
+                                z0=lims[2][0], u=f(u_xyz)[(slice(None),) + cut], region=f(reg_xyz)[cut],
+                                u_scale=1e9)
+    for g, w in zip(got, (oPhase.ravel(), oStruc, u, region)):  # u: x * 1e9 (native u_scale) vs x / 1e-9
+        np.testing.assert_allclose(g, w, rtol=1e-15, atol=1e-15 * np.abs(w).max())
