@@ -109,6 +109,34 @@ QPD_API int qpd_pack_device(qpd_ctx* ctx, const double* oPhase, const double* oS
                     void* P, void* U, int8_t* phase, void* weight, void* wdense, int32_t dense, uint32_t* flags,
                     void* stream);
 
+/* Q-POP-FerroDyn fields on the device, in their file order (nz, ny, nx) with x fastest, float32
+ * as FerroDyn writes them, already cropped to the planned grid except for the material field. */
+typedef struct qpd_fields {
+    const float* P[3];         /* order-parameter components (nStruc of them), C/m^2 before p_scale */
+    const float* u[3];         /* displacement components before u_scale (FerroDyn: metres), or all NULL */
+    const float* phase;        /* nPhase planes of phase fractions, or NULL: one-hot from the material */
+    const float* region;       /* scattering weight, or NULL: 1 */
+    const int8_t* material;    /* (nz_full, ny, nx) material indices: the crop's columns, full stack */
+    int64_t nz_full, z0;       /* layers in the material stack; the crop's first layer in it */
+    int32_t n_material;        /* entries of dc and phase_of, 1 .. 64 */
+    const double* dc;          /* host: c_m(T) / aC_z - 1 per material */
+    const int32_t* phase_of;   /* host: phase index of each material, -1 if it does not scatter */
+    double ramp_dz;            /* layer spacing of the u_z ramp, nm */
+    double p_scale, u_scale;   /* 1 / OS0 and the metres -> nm factor (1e9) */
+} qpd_fields;
+
+/* Boundary-input preparation on the GPU: the packed kernel inputs (same outputs and flags as
+ * qpd_pack_device) straight from FerroDyn fields.  Transposes to (x, y, z), scales P and u, sets
+ * the phases one-hot over the scattering materials (or from the phase fractions), the weight
+ * region = (material scatters) x region, and adds the u_z reference ramp
+ * (cumsum_z dc[mat] - dc[mat] / 2) ramp_dz summed over the full material stack from layer 0 and
+ * cropped at z0.  Replaces the host preparation of src/python/cli.py:174-217 and the `columns`
+ * kernel of src/heffte/kernels.cuh:34-50; a material index outside the tables fails with
+ * QPD_ERR_ARG.  stream is a cudaStream_t (NULL: the legacy default stream); the call
+ * synchronises it. */
+QPD_API int qpd_pack_fields(qpd_ctx* ctx, const qpd_fields* fields, void* P, void* U, int8_t* phase, void* weight,
+                            void* wdense, int32_t dense, uint32_t* flags, void* stream);
+
 /* The hot path on device-resident packed inputs, asynchronous on `stream` (a cudaStream_t;
  * NULL: the legacy default stream): P, U, weight, wdense in the plan precision (weight NULL: 1; wdense
  * non-NULL selects dense mode and phase/weight are ignored); I_dev receives n float64.

@@ -31,7 +31,7 @@ SCHEDULES = {"fused": QPD_SCHED_FUSED, "plain": QPD_SCHED_PLAIN}
 
 # Every symbol include/qpopdiff.h declares.
 EXPORTS = ("qpd_create", "qpd_destroy", "qpd_last_error", "qpd_plan", "qpd_set_crystal", "qpd_run_host",
-           "qpd_pack_device", "qpd_run_device", "qpd_device_status", "qpd_workspace_bytes", "qpd_launch_count", "qpd_enable_timing",
+           "qpd_pack_device", "qpd_pack_fields", "qpd_run_device", "qpd_device_status", "qpd_workspace_bytes", "qpd_launch_count", "qpd_enable_timing",
            "qpd_stage_times", "qpd_run_device_noalloc", "qpd_axis_radices")
 
 # Kernel kinds of qpd_stage_times (QPD_K_*), in index order.
@@ -47,6 +47,13 @@ class QpdCrystal(ctypes.Structure):
     _fields_ = [("nAtom", c_int32), ("nPhase", c_int32), ("nStruc", c_int32), ("G", c_double * 3),
                 ("qC", c_double * 3), ("V", c_double), ("R", POINTER(c_double)), ("f_re", POINTER(c_double)),
                 ("f_im", POINTER(c_double)), ("su", POINTER(c_double))]
+
+
+class QpdFields(ctypes.Structure):
+    _fields_ = [("P", c_void_p * 3), ("u", c_void_p * 3), ("phase", c_void_p), ("region", c_void_p),
+                ("material", c_void_p), ("nz_full", c_int64), ("z0", c_int64), ("n_material", c_int32),
+                ("dc", POINTER(c_double)), ("phase_of", POINTER(c_int32)), ("ramp_dz", c_double),
+                ("p_scale", c_double), ("u_scale", c_double)]
 
 
 class QpdError(RuntimeError):
@@ -86,6 +93,8 @@ def load(path=None):
         "qpd_run_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
         "qpd_pack_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p, c_void_p, c_void_p, c_int32, POINTER(c_uint32), c_void_p]),
+        "qpd_pack_fields": (c_int, [c_void_p, POINTER(QpdFields), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_int32, POINTER(c_uint32), c_void_p]),
         "qpd_run_device": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p]),
         "qpd_device_status": (c_int, [c_void_p]),
@@ -127,5 +136,5 @@ def axis_radices(n):
     return list(buf[:k])
 
 
-__all__ = ["load", "check", "axis_radices", "QpdGrid", "QpdCrystal", "QpdError", "QpdValueError", "QpdMemoryError",
+__all__ = ["load", "check", "axis_radices", "QpdGrid", "QpdCrystal", "QpdFields", "QpdError", "QpdValueError", "QpdMemoryError",
            "EXPORTS", "KERNEL_KINDS", "PRECISIONS", "SCHEDULES", "c_int8"]

@@ -17,6 +17,7 @@
 
 #include "qpopdiff.h"
 #include "qpd_fast.cuh"
+#include "qpd_fields.cuh"
 #include "qpd_kernels.cuh"
 
 using namespace qpd;
@@ -1086,6 +1087,51 @@ int field_map(qpd_ctx* c, CUtensorMap* m, void* base, bool fp64, int64_t nz, int
 
 }  // namespace
 
+namespace {
+
+template <typename T>
+int pack_fields_t(qpd_ctx* c, const qpd_fields* in, void* P, void* U, int8_t* phase, void* weight, void* wdense,
+                  uint32_t* fd, cudaStream_t st) {
+    FieldsArgs<T> a;
+    std::memset(&a, 0, sizeof a);
+    for (int k = 0; k < c->nStruc; k++) a.P[k] = in->P[k];
+    if (in->u[0])
+        for (int k = 0; k < 3; k++) a.u[k] = in->u[k];
+    a.phase = in->phase;
+    a.region = in->region;
+    a.mat = reinterpret_cast<const signed char*>(in->material);
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.nz = c->nz;
+    a.z0 = in->z0;
+    a.nStruc = c->nStruc;
+    a.nPhase = c->nPhase;
+    a.nMat = in->n_material;
+    a.dz = in->ramp_dz;
+    a.p_scale = in->p_scale;
+    a.u_scale = in->u_scale;
+    for (int m = 0; m < in->n_material; m++) {
+        a.dc[m] = in->dc[m];
+        a.phase_of[m] = (signed char)in->phase_of[m];
+    }
+    a.Pout = static_cast<T*>(P);
+    a.Uout = static_cast<T*>(U);
+    a.phase_idx = reinterpret_cast<signed char*>(phase);
+    a.weight = static_cast<T*>(weight);
+    a.wdense = static_cast<T*>(wdense);
+    a.flags = fd;
+    const int planes = c->nStruc + (in->u[0] ? 3 : 0) + (in->phase ? c->nPhase : 0) + (in->region ? 1 : 0);
+    const size_t smem = fields_smem_bytes(planes);
+    QPD_CU(c, cudaFuncSetAttribute(fields_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaEvent_t t0;
+    QPD_TRY(tstart(c, st, &t0));
+    dim3 grid((unsigned)((c->nx + kFT - 1) / kFT), (unsigned)c->ny);
+    fields_kernel<T><<<grid, dim3(kFT, kFRows), smem, st>>>(a);
+    return tstop(c, QPD_K_PACK, st, t0);
+}
+
+}  // namespace
+
 extern "C" {
 
 int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
@@ -1247,6 +1293,41 @@ int qpd_pack_device(qpd_ctx* c, const double* oPhase, const double* oStruc, cons
     uint32_t f = 0;
     QPD_CU(c, cudaMemcpyAsync(&f, fd, sizeof f, cudaMemcpyDeviceToHost, st));
     QPD_CU(c, cudaStreamSynchronize(st));
+    if (flags) *flags = f;
+    return QPD_OK;
+}
+
+int qpd_pack_fields(qpd_ctx* c, const qpd_fields* in, void* P, void* U, int8_t* phase, void* weight, void* wdense,
+                    int32_t dense, uint32_t* flags, void* stream) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_pack_fields: ctx is NULL");
+    if (!c->planned) return fail(c, QPD_ERR_STATE, "qpd_pack_fields before qpd_plan");
+    if (!in || !in->material || !in->dc || !in->phase_of) return fail(c, QPD_ERR_ARG, "qpd_pack_fields: NULL fields or tables");
+    for (int k = 0; k < c->nStruc; k++)
+        if (!in->P[k]) return fail(c, QPD_ERR_ARG, "qpd_pack_fields: P[%d] is NULL", k);
+    if ((in->u[0] != nullptr) != (in->u[1] != nullptr) || (in->u[0] != nullptr) != (in->u[2] != nullptr))
+        return fail(c, QPD_ERR_ARG, "qpd_pack_fields: give all three displacement components or none");
+    if (!P || !U || (dense ? !wdense : (!phase || !weight))) return fail(c, QPD_ERR_ARG, "qpd_pack_fields: NULL output");
+    if (in->n_material < 1 || in->n_material > kMaxMaterials)
+        return fail(c, QPD_ERR_ARG, "qpd_pack_fields: n_material %d outside 1..%d", in->n_material, kMaxMaterials);
+    for (int m = 0; m < in->n_material; m++)
+        if (in->phase_of[m] < -1 || in->phase_of[m] >= c->nPhase)
+            return fail(c, QPD_ERR_ARG, "qpd_pack_fields: phase_of[%d] = %d outside -1..%d", m, in->phase_of[m], c->nPhase - 1);
+    if (c->ny > 65535) return fail(c, QPD_ERR_UNSUPPORTED, "qpd_pack_fields: ny %lld > 65535", (long long)c->ny);
+    if (in->z0 < 0 || in->z0 + c->nz > in->nz_full)
+        return fail(c, QPD_ERR_ARG, "qpd_pack_fields: crop z0 %lld + nz %lld outside the %lld-layer stack",
+                    (long long)in->z0, (long long)c->nz, (long long)in->nz_full);
+    QPD_TRY(use_device(c));
+    QPD_TRY(dev_reserve(c, c->flags, 256, "flags"));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint32_t* fd = static_cast<uint32_t*>(c->flags.p);
+    QPD_CU(c, cudaMemsetAsync(fd, 0, sizeof(uint32_t), st));
+    int r = c->precision == QPD_FP64 ? pack_fields_t<double>(c, in, P, U, phase, weight, dense ? wdense : nullptr, fd, st)
+                                     : pack_fields_t<float>(c, in, P, U, phase, weight, dense ? wdense : nullptr, fd, st);
+    QPD_TRY(r);
+    uint32_t f = 0;
+    QPD_CU(c, cudaMemcpyAsync(&f, fd, sizeof f, cudaMemcpyDeviceToHost, st));
+    QPD_CU(c, cudaStreamSynchronize(st));
+    if (f & kFlagBadMaterial) return fail(c, QPD_ERR_ARG, "qpd_pack_fields: a material index lies outside the dc / phase_of tables");
     if (flags) *flags = f;
     return QPD_OK;
 }

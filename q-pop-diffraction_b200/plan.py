@@ -228,6 +228,86 @@ class Plan:
             return {"P": P, "U": U, "phase": None, "weight": None, "wdense": wdense}
         return {"P": P, "U": U, "phase": phase, "weight": weight if flags.value & 2 else None, "wdense": None}
 
+    def pack_fields(self, P, material, dc, phase_of, ramp_dz, z0=0, u=None, phase=None, region=None,
+                    p_scale=1.0, u_scale=1e9, stream=None):
+        """
+        Pack Q-POP-FerroDyn fields resident on the GPU into kernel inputs (qpd_pack_fields): the
+        preparation of src/python/cli.py:174-217 on the device.
+
+        P (nStruc planes), u (3 planes, metres; None: 0), phase (nPhase planes; None: one-hot from
+        the material) and region (None: 1) are float32 CUDA tensors in file order (nz, ny, nx),
+        cropped to the plan's grid; material is int8 (nz_full, ny, nx): the crop's columns over the
+        full stack, of which the crop starts at layer z0.  dc and phase_of are per-material tables
+        (c_m / aC_z - 1; phase index or -1).  Returns the same dict as pack().
+        """
+        import torch
+        dev = torch.device("cuda", self.device)
+        nx, ny, nz = self.shape
+        plane = nz * ny * nx
+        keep = []
+
+        def f32(t, count, name):
+            if t.dtype != torch.float32 or t.device != dev or t.numel() != count:
+                raise ValueError(f"{name}: expected {count} float32 values on {dev} in (nz, ny, nx) order")
+            t = t.contiguous()
+            keep.append(t)
+            return t.data_ptr()
+
+        def planes(ts, k, name):
+            if isinstance(ts, torch.Tensor):
+                ts = [ts[i] for i in range(ts.shape[0])] if ts.dim() == 4 else [ts]
+            if len(ts) < k:
+                raise ValueError(f"{name}: expected {k} planes")
+            return [f32(t, plane, f"{name}[{i}]") for i, t in enumerate(ts[:k])]
+
+        fields = nat.QpdFields()
+        for i, ptr in enumerate(planes(P, self.nStruc, "P") if self.nStruc else []):
+            fields.P[i] = ptr
+        if u is not None:
+            for i, ptr in enumerate(planes(u, 3, "u")):
+                fields.u[i] = ptr
+        if phase is not None:
+            fields.phase = f32(phase, self.nPhase * plane, "phase")
+        if region is not None:
+            fields.region = f32(region, plane, "region")
+        if material.dtype != torch.int8 or material.device != dev or material.dim() != 3 or \
+                tuple(material.shape[1:]) != (ny, nx):
+            raise ValueError(f"material: expected an int8 (nz_full, {ny}, {nx}) tensor on {dev}")
+        material = material.contiguous()
+        keep.append(material)
+        fields.material = material.data_ptr()
+        fields.nz_full, fields.z0 = int(material.shape[0]), int(z0)
+        dc = np.ascontiguousarray(dc, dtype=np.float64)
+        phase_of = np.ascontiguousarray(phase_of, dtype=np.int32)
+        if dc.shape != phase_of.shape or dc.ndim != 1:
+            raise ValueError("dc and phase_of: one entry per material")
+        fields.n_material = int(dc.size)
+        fields.dc = dc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        fields.phase_of = phase_of.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        fields.ramp_dz, fields.p_scale, fields.u_scale = float(ramp_dz), float(p_scale), float(u_scale)
+
+        n = self.n
+        dt = self.torch_dtype
+        Pout = torch.empty(3 * n, dtype=dt, device=dev)
+        Uout = torch.empty(3 * n, dtype=dt, device=dev)
+        phase_idx = torch.empty(n, dtype=torch.int8, device=dev)
+        weight = torch.empty(n, dtype=dt, device=dev)
+        flags = ctypes.c_uint32(0)
+        st = ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream)
+
+        def call(dense, wd):
+            self._check(self.lib.qpd_pack_fields(
+                self._ctx, ctypes.byref(fields), ctypes.c_void_p(Pout.data_ptr()), ctypes.c_void_p(Uout.data_ptr()),
+                ctypes.c_void_p(phase_idx.data_ptr()), ctypes.c_void_p(weight.data_ptr()),
+                ctypes.c_void_p(wd.data_ptr()) if wd is not None else None, int(dense), ctypes.byref(flags), st))
+
+        call(False, None)
+        if flags.value & 1:
+            wdense = torch.empty(self.nPhase * n, dtype=dt, device=dev)
+            call(True, wdense)
+            return {"P": Pout, "U": Uout, "phase": None, "weight": None, "wdense": wdense}
+        return {"P": Pout, "U": Uout, "phase": phase_idx, "weight": weight if flags.value & 2 else None, "wdense": None}
+
     def run_device(self, inputs, out=None, stream=None):
         """Enqueue the hot path on device-resident packed inputs; returns the (nx, ny, nz) float64 tensor."""
         import torch
