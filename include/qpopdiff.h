@@ -173,6 +173,16 @@ QPD_API uint64_t qpd_launch_count(const qpd_ctx* ctx);
 QPD_API int qpd_enable_timing(qpd_ctx* ctx, int32_t on);
 QPD_API int qpd_stage_times(qpd_ctx* ctx, double* ms, uint64_t* counts, int32_t cap);
 
+/* Reciprocal-space-map projections of a device-resident intensity I (nx, ny, nz) float64, z
+ * fastest: xy[x * ny + y] = sum_z I, xz[x * nz + z] = sum_y I, yz[y * nz + z] = sum_x I (a NULL
+ * output is skipped).  Deterministic: fixed summation order, no atomics.  With the tensor-product
+ * q grid every map of src/python/rsm.py:88-104 (numpy.histogram2d of I over two broadcast q
+ * components) is one of these projections re-binned along its two 1-D axes, which the host does
+ * on the small maps.  No context: failures are described by qpd_last_error(NULL); ny <= 16384.
+ * Asynchronous on `stream` (NULL: the default stream). */
+QPD_API int qpd_rsm_project(const double* I, int64_t nx, int64_t ny, int64_t nz, double* xy, double* xz, double* yz,
+                            void* stream);
+
 /* Bytes of the device array behind qpd_run_device_noalloc. */
 #define QPD_NOALLOC_SCRATCH_BYTES (32u << 20)
 

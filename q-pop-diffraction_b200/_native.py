@@ -32,7 +32,7 @@ SCHEDULES = {"fused": QPD_SCHED_FUSED, "plain": QPD_SCHED_PLAIN}
 # Every symbol include/qpopdiff.h declares.
 EXPORTS = ("qpd_create", "qpd_destroy", "qpd_last_error", "qpd_plan", "qpd_set_crystal", "qpd_run_host",
            "qpd_pack_device", "qpd_pack_fields", "qpd_run_device", "qpd_device_status", "qpd_workspace_bytes", "qpd_launch_count", "qpd_enable_timing",
-           "qpd_stage_times", "qpd_run_device_noalloc", "qpd_axis_radices")
+           "qpd_stage_times", "qpd_run_device_noalloc", "qpd_rsm_project", "qpd_axis_radices")
 
 # Kernel kinds of qpd_stage_times (QPD_K_*), in index order.
 KERNEL_KINDS = ("zstage", "ypass", "xpass", "pack", "source", "fftz", "axis", "accumulate", "intensity")
@@ -104,6 +104,7 @@ def load(path=None):
         "qpd_stage_times": (c_int, [c_void_p, POINTER(c_double), POINTER(c_uint64), c_int32]),
         "qpd_run_device_noalloc": (c_int, [POINTER(QpdGrid), POINTER(QpdCrystal), c_void_p, c_void_p, c_void_p,
                                            c_void_p, c_void_p, c_void_p]),
+        "qpd_rsm_project": (c_int, [c_void_p, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
         "qpd_axis_radices": (c_int, [c_int64, POINTER(c_int32), c_int32]),
     }
     for name, (res, args) in sig.items():

@@ -21,7 +21,7 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 LIB = PKG / "libqpopdiff.so"
 
-SOURCES = ["qpd_api.cu", "qpd_noalloc.cu"]
+SOURCES = ["qpd_api.cu", "qpd_noalloc.cu", "qpd_rsm.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
