@@ -145,6 +145,17 @@ QPD_API int qpd_pack_fields(qpd_ctx* ctx, const qpd_fields* fields, void* P, voi
 QPD_API int qpd_run_device(qpd_ctx* ctx, const void* P, const void* U, const int8_t* phase, const void* weight,
                    const void* wdense, double* I_dev, void* stream);
 
+/* No counterpart in the reference (differentiation through the model): the gradient of a scalar
+ * loss L(I) with respect to the packed inputs.  dI holds dL/dI (n float64, the fftshifted
+ * layout of I); writes dL/dP (3 * n; planes beyond nStruc are 0) and dL/dU (3 * n) in the plan
+ * precision, for the same packed inputs as qpd_run_device (which need not have run: the forward is
+ * recomputed pass by pass, nothing is kept between the calls).  Voxels at the 1e-50 floor pass no
+ * gradient.  Fused schedule only (QPD_ERR_UNSUPPORTED otherwise); needs (1 + 2 G2) more complex
+ * fields of workspace, G2 the atoms' distinct R_x.  Asynchronous on `stream` (NULL: the legacy
+ * default stream). */
+QPD_API int qpd_adjoint_device(qpd_ctx* ctx, const void* P, const void* U, const int8_t* phase, const void* weight,
+                               const void* wdense, const double* dI, void* dP, void* dU, void* stream);
+
 /* Wait for the device and report whether a kernel of this context gave up on a bounded wait
  * (a tile load that never completed): QPD_OK, or QPD_ERR_CUDA with the status cleared.
  * qpd_run_host checks this itself; callers of qpd_run_device call it after synchronising. */
@@ -164,7 +175,10 @@ QPD_API uint64_t qpd_launch_count(const qpd_ctx* ctx);
 #define QPD_K_AXIS 6     /* plain: y or x transform */
 #define QPD_K_ACC 7      /* plain: amplitude update */
 #define QPD_K_INTENSITY 8 /* plain: intensity + fftshift */
-#define QPD_K_COUNT 9
+#define QPD_K_ADJSEED 9  /* adjoint: x pass of the recomputed forward, seeding dL/dconj(Amp) */
+#define QPD_K_ADJAXIS 10 /* adjoint: x or y pass */
+#define QPD_K_ADJZ 11    /* adjoint: z transform + source transpose */
+#define QPD_K_COUNT 12
 
 /* Per-kernel timing: while on, CUDA events are recorded around every kernel the context
  * launches.  qpd_stage_times waits for them, writes the summed device milliseconds and the

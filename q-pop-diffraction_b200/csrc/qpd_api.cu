@@ -62,9 +62,12 @@ struct qpd_ctx {
     size_t off_apc = 0, off_coefE = 0, off_coefUz = 0, off_S[3] = {0, 0, 0}, off_segY = 0, off_segX = 0;
     size_t off_pex = 0, off_pey = 0, off_pez = 0, off_k[3] = {0, 0, 0};
     int nsegY = 0;
+    size_t off_segAX = 0, off_segAY = 0;  // adjoint passes
+    int nsegAX = 0, nsegAY = 0;
 
     // workspace
     DevMem fields;  // fused: 3 * ng1 fields; plain: buf + amp
+    DevMem adjw;    // adjoint: the seed D and 2 * ng2 fields after the adjoint x pass
     DevMem packed;  // host path: P, U, phase, weight
     DevMem dense;   // host path, dense weights
     DevMem stage;   // host path, float64 staging
@@ -377,7 +380,7 @@ template <typename T> struct Impl {
             c->off_S[d] = place(sizeof(double) * N[d]);
             std::memcpy(host.data() + c->off_S[d], S[d].data(), sizeof(double) * N[d]);
         }
-        std::vector<Segment<T>> segY, segX;
+        std::vector<Segment<T>> segY, segX, segAX, segAY;
         if (sched == QPD_SCHED_FUSED) {
             c->off_coefE = place(sizeof(C) * A * N[2]);
             c->off_coefUz = place(sizeof(C) * A * N[2]);
@@ -450,6 +453,32 @@ template <typename T> struct Impl {
             c->nsegY = 2 * G2;
             c->off_segY = place(sizeof(Segment<T>) * segY.size());
             c->off_segX = place(sizeof(Segment<T>));
+            // adjoint x pass: adjoint workspace slot 0 (the seed) -> slots 1 + 2 g2 (ex) and 2 + 2 g2 (-i k_x ex);
+            // adjoint y pass: slot 1 + 2 g2 -> fields 3 g1 (ey) and 3 g1 + 2 (-i k_y ey), slot 2 + 2 g2 -> 3 g1 + 1 (ey)
+            auto one = [](int in, size_t coef, int out) {
+                Segment<T> t;
+                std::memset(&t, 0, sizeof t);
+                t.nin = 1;
+                t.nout = 1;
+                t.in[0] = in;
+                t.coef[0][0] = reinterpret_cast<const C*>(coef + 1);
+                t.out[0] = out;
+                return t;
+            };
+            for (int g2 = 0; g2 < G2; g2++) {
+                segAX.push_back(one(0, offX[g2], 1 + 2 * g2));
+                segAX.push_back(one(0, offX[g2] + sizeof(C) * N[0], 2 + 2 * g2));
+            }
+            for (int g1 = 0; g1 < G1; g1++) {
+                const int g2 = g2of[g1];
+                segAY.push_back(one(1 + 2 * g2, offY[g1], 3 * g1));
+                segAY.push_back(one(1 + 2 * g2, offY[g1] + sizeof(C) * N[1], 3 * g1 + 2));
+                segAY.push_back(one(2 + 2 * g2, offY[g1], 3 * g1 + 1));
+            }
+            c->nsegAX = (int)segAX.size();
+            c->nsegAY = (int)segAY.size();
+            c->off_segAX = place(sizeof(Segment<T>) * segAX.size());
+            c->off_segAY = place(sizeof(Segment<T>) * segAY.size());
         } else {
             // plain: per-atom axis factors in double and the wavenumbers
             c->off_pex = place(sizeof(double2) * A * N[0]);
@@ -482,7 +511,11 @@ template <typename T> struct Impl {
         };
         for (auto& s : segY) fix(s);
         for (auto& s : segX) fix(s);
+        for (auto& s : segAX) fix(s);
+        for (auto& s : segAY) fix(s);
         if (!segY.empty()) std::memcpy(host.data() + c->off_segY, segY.data(), sizeof(Segment<T>) * segY.size());
+        if (!segAX.empty()) std::memcpy(host.data() + c->off_segAX, segAX.data(), sizeof(Segment<T>) * segAX.size());
+        if (!segAY.empty()) std::memcpy(host.data() + c->off_segAY, segAY.data(), sizeof(Segment<T>) * segAY.size());
         std::memcpy(host.data() + c->off_segX, segX.data(), sizeof(Segment<T>));
         QPD_CU(c, cudaMemcpyAsync(c->tables.p, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
         QPD_CU(c, cudaStreamSynchronize(c->stream));
@@ -553,7 +586,7 @@ template <typename T> struct Impl {
         return fail(c, QPD_ERR_UNSUPPORTED, "nz = %d is too long for the z transform in this precision", a.nz);
     }
 
-    template <int NT, int EPT, bool EPI>
+    template <int NT, int EPT, int EPI>
     static int launch_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
         a.Cz = std::max(1, std::min(a.nz, NT * EPT / a.N));
         a.nzc = (a.nz + a.Cz - 1) / a.Cz;
@@ -566,7 +599,7 @@ template <typename T> struct Impl {
         return tstop(c, kind, st, t0);
     }
 
-    template <bool EPI> static int run_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+    template <int EPI> static int run_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
         const size_t lim = max_smem(c);
         int best = -1, bestCz = 0;
         for (int i = 0; i < 4; i++) {
@@ -588,6 +621,70 @@ template <typename T> struct Impl {
             case 3: return launch_axis<1024, 16, EPI>(c, a, nouter, kind, st);
         }
         return fail(c, QPD_ERR_UNSUPPORTED, "an axis of length %d is too long in this precision", a.N);
+    }
+
+    // ---------------- adjoint (generic kernels) ----------------
+    template <int NT, int EPT> static int launch_adj_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, cudaStream_t st) {
+        a.Cz = std::max(1, std::min(a.nz, NT * EPT / a.N));
+        a.nzc = (a.nz + a.Cz - 1) / a.Cz;
+        const size_t smem = sizeof(C) * a.N * a.Cz + 16;
+        QPD_TRY(set_smem(c, adj_axis_kernel<T, NT, EPT>, smem));
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        adj_axis_kernel<T, NT, EPT><<<(unsigned)(nouter * a.nzc), NT, smem, st>>>(a);
+        return tstop(c, QPD_K_ADJAXIS, st, t0);
+    }
+
+    static int run_adj_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, cudaStream_t st) {
+        const size_t lim = max_smem(c);
+        int best = -1, bestCz = 0;
+        for (int i = 0; i < 4; i++) {
+            const Cfg& f = kACfg[i];
+            const int cap = f.nt * f.ept;
+            if (a.N > cap) continue;
+            const int Cz = std::min(a.nz, cap / a.N);
+            if (sizeof(C) * a.N * Cz + 16 > lim) continue;
+            if (best < 0 || std::min(Cz, 8) > std::min(bestCz, 8)) {
+                best = i;
+                bestCz = Cz;
+            }
+        }
+        switch (best) {
+            case 0: return launch_adj_axis<256, 16>(c, a, nouter, st);
+            case 1: return launch_adj_axis<512, 16>(c, a, nouter, st);
+            case 2: return launch_adj_axis<1024, 8>(c, a, nouter, st);
+            case 3: return launch_adj_axis<1024, 16>(c, a, nouter, st);
+        }
+        return fail(c, QPD_ERR_UNSUPPORTED, "an axis of length %d is too long for the adjoint in this precision", a.N);
+    }
+
+    template <int NT, int EPT> static int launch_adj_z(qpd_ctx* c, AdjZArgs<T>& a, cudaStream_t st) {
+        const int cap = NT * EPT / 4;
+        a.z.M = std::max(1, (int)std::min<int64_t>(cap / a.z.nz, a.z.ncols));
+        a.z.ps = odd_stride(a.z.nz);
+        const size_t smem = sizeof(C) * 4 * a.z.M * a.z.ps + sizeof(AtomPhase<T>) * a.z.in.nPhase * a.z.nAtom + 16;
+        QPD_TRY(set_smem(c, adj_zstage_kernel<T, NT, EPT>, smem));
+        const int64_t grid = (a.z.ncols + a.z.M - 1) / a.z.M;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        adj_zstage_kernel<T, NT, EPT><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_ADJZ, st, t0);
+    }
+
+    static int run_adj_z(qpd_ctx* c, AdjZArgs<T>& a, cudaStream_t st) {
+        const size_t lim = max_smem(c);
+        for (const Cfg& f : kZCfg) {
+            const int cap = f.nt * f.ept / 4;
+            if (a.z.nz > cap) continue;
+            const int M = std::max(1, (int)std::min<int64_t>(cap / a.z.nz, a.z.ncols));
+            const size_t smem = sizeof(C) * 4 * M * odd_stride(a.z.nz) + sizeof(AtomPhase<T>) * a.z.in.nPhase * a.z.nAtom + 16;
+            if (smem > lim) continue;
+            if (f.nt == 256 && f.ept == 16) return launch_adj_z<256, 16>(c, a, st);
+            if (f.nt == 512 && f.ept == 16) return launch_adj_z<512, 16>(c, a, st);
+            if (f.nt == 1024 && f.ept == 8) return launch_adj_z<1024, 8>(c, a, st);
+            if (f.nt == 1024 && f.ept == 16) return launch_adj_z<1024, 16>(c, a, st);
+        }
+        return fail(c, QPD_ERR_UNSUPPORTED, "nz = %d is too long for the adjoint z stage in this precision", a.z.nz);
     }
 
     // ---------------- compile-time specialised kernels ----------------
@@ -755,25 +852,103 @@ template <typename T> struct Impl {
         return in;
     }
 
-    static int run_device(qpd_ctx* c, const Inputs<T>& in, double* I, cudaStream_t st) {
+    // fused z stage (source + z transform + fold) and y pass, leaving 2 ng2 fields in c->fields
+    static ZArgs<T> zargs(qpd_ctx* c, const Inputs<T>& in) {
+        ZArgs<T> z;
+        std::memset(&z, 0, sizeof z);
+        z.in = in;
+        z.ncols = c->nx * c->ny;
+        z.nz = (int)c->nz;
+        z.nAtom = c->nAtom;
+        z.apc = tab<AtomPhase<T>>(c, c->off_apc);
+        z.coefE = tab<C>(c, c->off_coefE);
+        z.coefUz = tab<C>(c, c->off_coefUz);
+        for (int i = 0; i < c->nAtom; i++) z.grp[i] = c->grp[i];
+        z.out = static_cast<C*>(c->fields.p);
+        z.fstride = c->n;
+        for (int d = 0; d < 3; d++) z.tq[d] = c->tq[d];
+        z.zp = axis_plan(c, 2);
+        z.status = static_cast<int*>(c->status.p);
+        return z;
+    }
+
+    static AxisArgs<T> xargs(qpd_ctx* c) {
+        AxisArgs<T> x;
+        std::memset(&x, 0, sizeof x);
+        x.N = (int)c->nx;
+        x.stride = c->ny * c->nz;
+        x.ostride = c->nz;
+        x.nz = (int)c->nz;
+        x.in = static_cast<C*>(c->fields.p);
+        x.fstride = c->n;
+        x.segs = tab<Segment<T>>(c, c->off_segX);
+        x.nseg = 1;
+        x.ap = axis_plan(c, 0);
+        for (int d = 0; d < 3; d++) x.S[d] = tab<double>(c, c->off_S[d]);
+        x.scale2 = c->scale2;
+        x.nx = c->nx;
+        x.ny = c->ny;
+        x.status = static_cast<int*>(c->status.p);
+        return x;
+    }
+
+    // Gradient of a loss through the fused schedule: recompute the forward to the x pass, seed,
+    // then the adjoint x, y and z passes (the last fused with the source transpose).
+    static int adjoint(qpd_ctx* c, const Inputs<T>& in, const double* dI, T* dP, T* dU, cudaStream_t st) {
+        const int64_t n = c->n;
+        QPD_TRY(dev_reserve(c, c->adjw, sizeof(C) * (size_t)(1 + 2 * c->ng2) * n, "adjoint workspace"));
+        C* F = static_cast<C*>(c->fields.p);
+        C* W = static_cast<C*>(c->adjw.p);
+        QPD_TRY(forward_zy(c, in, st));
+
+        AxisArgs<T> x = xargs(c);
+        x.out = W;
+        x.gI = dI;
+        QPD_TRY(run_axis<2>(c, x, c->ny, QPD_K_ADJSEED, st));
+
+        AxisArgs<T> ax;
+        std::memset(&ax, 0, sizeof ax);
+        ax.N = (int)c->nx;
+        ax.stride = c->ny * c->nz;
+        ax.ostride = c->nz;
+        ax.nz = (int)c->nz;
+        ax.in = W;
+        ax.out = W;
+        ax.fstride = n;
+        ax.segs = tab<Segment<T>>(c, c->off_segAX);
+        ax.nseg = c->nsegAX;
+        ax.ap = axis_plan(c, 0);
+        QPD_TRY(run_adj_axis(c, ax, c->ny, st));
+
+        AxisArgs<T> ay;
+        std::memset(&ay, 0, sizeof ay);
+        ay.N = (int)c->ny;
+        ay.stride = c->nz;
+        ay.ostride = c->ny * c->nz;
+        ay.nz = (int)c->nz;
+        ay.in = W;
+        ay.out = F;
+        ay.fstride = n;
+        ay.segs = tab<Segment<T>>(c, c->off_segAY);
+        ay.nseg = c->nsegAY;
+        ay.ap = axis_plan(c, 1);
+        QPD_TRY(run_adj_axis(c, ay, c->nx, st));
+
+        AdjZArgs<T> az;
+        std::memset(&az, 0, sizeof az);
+        az.z = zargs(c, in);
+        az.fin = F;
+        az.dU = dU;
+        az.dP = dP;
+        for (int d = 0; d < 3; d++) az.qc[d] = 2.0 * M_PI * c->tq[d];
+        return run_adj_z(c, az, st);
+    }
+
+    static int forward_zy(qpd_ctx* c, const Inputs<T>& in, cudaStream_t st) {
         C* F = static_cast<C*>(c->fields.p);
         const int64_t n = c->n;
-        if (c->sched_used == QPD_SCHED_FUSED) {
-            ZArgs<T> z;
-            std::memset(&z, 0, sizeof z);
-            z.in = in;
-            z.ncols = c->nx * c->ny;
-            z.nz = (int)c->nz;
-            z.nAtom = c->nAtom;
-            z.apc = tab<AtomPhase<T>>(c, c->off_apc);
-            z.coefE = tab<C>(c, c->off_coefE);
-            z.coefUz = tab<C>(c, c->off_coefUz);
-            for (int i = 0; i < c->nAtom; i++) z.grp[i] = c->grp[i];
-            z.out = F;
-            z.fstride = n;
-            for (int d = 0; d < 3; d++) z.tq[d] = c->tq[d];
-            z.zp = axis_plan(c, 2);
-            z.status = static_cast<int*>(c->status.p);
+        {
+            ZArgs<T> z = zargs(c, in);
             bool done = false;
             if (c->fast) QPD_TRY(fast_z(c, z, st, &done));
             if (!done) QPD_TRY(run_z(c, z, st));
@@ -795,29 +970,22 @@ template <typename T> struct Impl {
             y.status = static_cast<int*>(c->status.p);
             done = false;
             if (c->fast) QPD_TRY(fast_axis<false>(c, y, c->nx, QPD_K_YPASS, st, &done));
-            if (!done) QPD_TRY(run_axis<false>(c, y, c->nx, QPD_K_YPASS, st));
+            if (!done) QPD_TRY(run_axis<0>(c, y, c->nx, QPD_K_YPASS, st));
+        }
+        return QPD_OK;
+    }
 
-            AxisArgs<T> x;
-            std::memset(&x, 0, sizeof x);
-            x.N = (int)c->nx;
-            x.stride = c->ny * c->nz;
-            x.ostride = c->nz;
-            x.nz = (int)c->nz;
-            x.in = F;
-            x.fstride = n;
-            x.segs = tab<Segment<T>>(c, c->off_segX);
-            x.nseg = 1;
-            x.ap = axis_plan(c, 0);
+    static int run_device(qpd_ctx* c, const Inputs<T>& in, double* I, cudaStream_t st) {
+        C* F = static_cast<C*>(c->fields.p);
+        const int64_t n = c->n;
+        if (c->sched_used == QPD_SCHED_FUSED) {
+            QPD_TRY(forward_zy(c, in, st));
+            AxisArgs<T> x = xargs(c);
             x.I = I;
-            for (int d = 0; d < 3; d++) x.S[d] = tab<double>(c, c->off_S[d]);
-            x.scale2 = c->scale2;
-            x.nx = c->nx;
-            x.ny = c->ny;
-            x.status = static_cast<int*>(c->status.p);
-            done = false;
+            bool done = false;
             if (c->fast) QPD_TRY(fast_axis<true>(c, x, c->ny, QPD_K_XPASS, st, &done));
             if (done) return QPD_OK;
-            return run_axis<true>(c, x, c->ny, QPD_K_XPASS, st);
+            return run_axis<1>(c, x, c->ny, QPD_K_XPASS, st);
         }
         // plain schedule
         C* buf = F;
@@ -864,7 +1032,7 @@ template <typename T> struct Impl {
                     ax.nx = c->nx;
                     ax.ny = c->ny;
                     ax.status = static_cast<int*>(c->status.p);
-                    QPD_TRY(run_axis<false>(c, ax, d == 1 ? c->nx : c->ny, QPD_K_AXIS, st));
+                    QPD_TRY(run_axis<0>(c, ax, d == 1 ? c->nx : c->ny, QPD_K_AXIS, st));
                 }
 
                 AccArgs<T> ac;
@@ -1345,6 +1513,23 @@ int qpd_run_device(qpd_ctx* c, const void* P, const void* U, const int8_t* phase
     }
     Inputs<float> in = Impl<float>::inputs(c, P, U, phase, weight, wdense);
     return Impl<float>::run_device(c, in, I_dev, st);
+}
+
+int qpd_adjoint_device(qpd_ctx* c, const void* P, const void* U, const int8_t* phase, const void* weight,
+                       const void* wdense, const double* dI, void* dP, void* dU, void* stream) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_adjoint_device: ctx is NULL");
+    if (!c->planned || !c->have_crystal) return fail(c, QPD_ERR_STATE, "qpd_adjoint_device needs qpd_plan and qpd_set_crystal");
+    if (!P || !U || !dI || !dP || !dU || (!wdense && !phase)) return fail(c, QPD_ERR_ARG, "qpd_adjoint_device: NULL array");
+    if (c->sched_used != QPD_SCHED_FUSED)
+        return fail(c, QPD_ERR_UNSUPPORTED, "qpd_adjoint_device: the adjoint runs on the fused schedule only");
+    QPD_TRY(use_device(c));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (c->precision == QPD_FP64) {
+        Inputs<double> in = Impl<double>::inputs(c, P, U, phase, weight, wdense);
+        return Impl<double>::adjoint(c, in, dI, static_cast<double*>(dP), static_cast<double*>(dU), st);
+    }
+    Inputs<float> in = Impl<float>::inputs(c, P, U, phase, weight, wdense);
+    return Impl<float>::adjoint(c, in, dI, static_cast<float*>(dP), static_cast<float*>(dU), st);
 }
 
 int qpd_enable_timing(qpd_ctx* c, int32_t on) {

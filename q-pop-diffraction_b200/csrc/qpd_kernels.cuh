@@ -303,9 +303,12 @@ template <typename T> struct AxisArgs {
     double scale2;      // (1 / (n V))^2
     long long nx, ny;
     int* status;        // device status word: bounded waits record timeouts here
+    const double* gI;   // adjoint seed (EPI 2): dL/dI, fftshifted like I
 };
 
-template <typename T, int NT, int EPT, bool EPI>
+// EPI 0: store the folded fields; 1: intensity epilogue; 2: adjoint seed, the conjugate gradient
+// D(k) = dL/dI S^2 conj(Amp) / (n V) written as field seg.out[0] (zero where I is at its floor).
+template <typename T, int NT, int EPT, int EPI>
 __global__ void __launch_bounds__(NT) axis_kernel(AxisArgs<T> a) {
     using C = C_t<T>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -356,7 +359,29 @@ __global__ void __launch_bounds__(NT) axis_kernel(AxisArgs<T> a) {
             }
             __syncthreads();
         }
-        if (EPI) {
+        if (EPI == 2) {
+            const long long ky = outer;
+            const long long sy = (ky + a.ny / 2) % a.ny;
+            const double syv = a.S[1][ky];
+            C* dst = a.out + seg.out[0] * a.fstride + base;
+#pragma unroll
+            for (int q = 0; q < EPT; q++) {
+                const int e = tid + q * NT;
+                if (e < ne) {
+                    const int kx = e / cz;
+                    const int c = e - kx * cz;
+                    const int kz = z0 + c;
+                    const double S = a.S[0][kx] * syv * a.S[2][kz];
+                    const double re = (double)acc[0][q].x, im = (double)acc[0][q].y;
+                    const double S2 = S * S * a.scale2;
+                    const long long sx = (kx + a.nx / 2) % a.nx;
+                    const long long sz = (kz + a.nz / 2) % a.nz;
+                    double f = 0.0;
+                    if (S2 * (re * re + im * im) > 1e-50) f = a.gI[(sx * a.ny + sy) * a.nz + sz] * S2;
+                    dst[kx * a.stride + c] = cmake<C>(T(f * re), T(-f * im));
+                }
+            }
+        } else if (EPI == 1) {
             const long long ky = outer;
             const long long sy = (ky + a.ny / 2) % a.ny;
             const double syv = a.S[1][ky];
@@ -395,6 +420,203 @@ __global__ void __launch_bounds__(NT) axis_kernel(AxisArgs<T> a) {
             }
         }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Adjoint (fused schedule).  With B = dL/dconj(Amp) = dL/dI S^2 Amp, the gradient of the
+// source fields is G = ifftn(conj(phi) B ...), phi the separable per-atom factors.  Its conjugate
+// conj(G) = fftn(phi conj(B)) / n runs the forward transforms with the forward tables, in the
+// reverse axis order, unfolding the groups instead of folding them:
+//   seed (axis_kernel, EPI 2)  D = dL/dI S^2 conj(Amp) / (n V)     (x pass of the recomputed forward)
+//   adj_axis_kernel (x)        per R_x group: ex D, -i k_x ex D     -> FFT along x
+//   adj_axis_kernel (y)        per (R_x, R_y) group: ey B, -i k_y ey B, ey X -> FFT along y
+//   adj_zstage_kernel          per atom: ez A, -i k_z ez A, ez X, ez Y -> FFT along z = conj(G_E),
+//                              conj(G_Uz), conj(G_Ux), conj(G_Uy), then the transpose of the source:
+//   h_c = 2 qC_c Im(Q) + 2 Re(e conj(G_Uc)),  Q = e (conj(G_E) + sum_d u_d conj(G_Ud)),
+//   e = w f exp(-i qC . u_ap);  dL/du_c += h_c,  dL/dP_s += sum_c su[c][s] h_c.
+// ---------------------------------------------------------------------------------------
+
+// out_o = FFT(sum_i coef[o][i](k) in_i(k)) along the axis: multiply first, then transform.
+template <typename T, int NT, int EPT>
+__global__ void __launch_bounds__(NT) adj_axis_kernel(AxisArgs<T> a) {
+    using C = C_t<T>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const int tid = threadIdx.x;
+    const long long outer = blockIdx.x / a.nzc;
+    const int z0 = (int)(blockIdx.x % a.nzc) * a.Cz;
+    const int cz = min(a.Cz, a.nz - z0);
+    const int ne = a.N * cz;
+    const long long base = outer * a.ostride + z0;
+    const Pencils pg{cz, cz, 0, 1, a.Cz};
+    for (int sg = 0; sg < a.nseg; sg++) {
+        const Segment<T>& seg = a.segs[sg];
+        C acc[EPT];
+#pragma unroll
+        for (int q = 0; q < EPT; q++) acc[q] = cmake<C>(0, 0);
+        for (int fi = 0; fi < seg.nin; fi++) {
+            const C* src = a.in + seg.in[fi] * a.fstride + base;
+            const C* cf = seg.coef[0][fi];
+#pragma unroll
+            for (int q = 0; q < EPT; q++) {
+                const int e = tid + q * NT;
+                if (e < ne) {
+                    const int k = e / cz;
+                    const int c = e - k * cz;
+                    cfma(acc[q], cf[k], src[k * a.stride + c]);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < EPT; q++) {
+            const int e = tid + q * NT;
+            if (e < ne) {
+                const int k = e / cz;
+                buf[k * a.Cz + (e - k * cz)] = acc[q];
+            }
+        }
+        __syncthreads();
+        fft_pencils<T, EPT>(buf, pg, a.ap, tid, NT);
+        C* dst = a.out + seg.out[0] * a.fstride + base;
+#pragma unroll
+        for (int q = 0; q < EPT; q++) {
+            const int e = tid + q * NT;
+            if (e < ne) {
+                const int i = e / cz;
+                const int c = e - i * cz;
+                dst[i * a.stride + c] = buf[i * a.Cz + c];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Transpose of add_source: accumulate the gradient of one (phase, atom) term at a cell.
+template <typename T>
+__device__ __forceinline__ void add_adjoint(const CellIn<T>& c, const AtomPhase<T>& k, T w, const double qc[3],
+                                            C_t<T> gE, C_t<T> gX, C_t<T> gY, C_t<T> gZ, T dU[3], T dP[3]) {
+    double t = c.tu + k.bq[0] * (double)c.p[0] + k.bq[1] * (double)c.p[1] + k.bq[2] * (double)c.p[2];
+    t -= rint(t);
+    T sn, cs;
+    expm2pi(t, &sn, &cs);
+    const T er = w * (k.fr * cs + k.fi * sn);
+    const T ei = w * (k.fi * cs - k.fr * sn);
+    const T ua0 = c.u[0] + k.su[0] * c.p[0] + k.su[1] * c.p[1] + k.su[2] * c.p[2];
+    const T ua1 = c.u[1] + k.su[3] * c.p[0] + k.su[4] * c.p[1] + k.su[5] * c.p[2];
+    const T ua2 = c.u[2] + k.su[6] * c.p[0] + k.su[7] * c.p[1] + k.su[8] * c.p[2];
+    // s = conj(G_E) + sum_d u_d conj(G_Ud);  Im(Q) = Im(e s)
+    const T sr = gE.x + ua0 * gX.x + ua1 * gY.x + ua2 * gZ.x;
+    const T si = gE.y + ua0 * gX.y + ua1 * gY.y + ua2 * gZ.y;
+    const T imq = er * si + ei * sr;
+    T h[3];
+    h[0] = T(2) * (T(qc[0]) * imq + er * gX.x - ei * gX.y);
+    h[1] = T(2) * (T(qc[1]) * imq + er * gY.x - ei * gY.y);
+    h[2] = T(2) * (T(qc[2]) * imq + er * gZ.x - ei * gZ.y);
+#pragma unroll
+    for (int d = 0; d < 3; d++) dU[d] += h[d];
+#pragma unroll
+    for (int s = 0; s < 3; s++) dP[s] += k.su[s] * h[0] + k.su[3 + s] * h[1] + k.su[6 + s] * h[2];
+}
+
+template <typename T> struct AdjZArgs {
+    ZArgs<T> z;             // inputs, tables, groups; z.out unused
+    const C_t<T>* fin;      // conjugate adjoint fields after the y pass: 3 g + {0: A, 1: X, 2: Y}
+    T* dU;                  // 3 planes of n
+    T* dP;                  // 3 planes of n
+    double qc[3];           // qC
+};
+
+template <typename T, int NT, int EPT>
+__global__ void __launch_bounds__(NT) adj_zstage_kernel(AdjZArgs<T> a) {
+    using C = C_t<T>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const ZArgs<T>& z = a.z;
+    const int plane = z.M * z.ps;
+    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(buf + 4 * plane);
+    const int tid = threadIdx.x;
+    const int nap = z.in.nPhase * z.nAtom;
+    for (int i = tid; i < nap; i += NT) apc[i] = z.apc[i];
+
+    constexpr int CPT = EPT / 4;
+    const long long c0 = (long long)blockIdx.x * z.M;
+    const int mcols = (int)min((long long)z.M, z.ncols - c0);
+    const int ncell = mcols * z.nz;
+    const long long g0 = c0 * z.nz;
+    const long long n = z.in.n;
+
+    CellIn<T> cell[CPT];
+    int ph[CPT];
+    T wt[CPT], dU[CPT][3], dP[CPT][3];
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int e = tid + q * NT;
+        ph[q] = -1;
+        wt[q] = T(0);
+        for (int d = 0; d < 3; d++) dU[q][d] = dP[q][d] = T(0);
+        if (e < ncell) {
+            const long long g = g0 + e;
+            load_cell<T>(z.in, g, z.tq, cell[q]);
+            if (!z.in.wdense) {
+                ph[q] = z.in.phase[g];
+                wt[q] = z.in.weight ? z.in.weight[g] : T(1);
+            }
+        }
+    }
+    const Pencils pg{4 * z.M, 4 * z.M, 0, z.ps, 1};
+    __syncthreads();
+    for (int at = 0; at < z.nAtom; at++) {
+        const int g = z.grp[at];
+        const C* fa = a.fin + 3LL * g * z.fstride + g0;
+        const C* ce = z.coefE + (long long)at * z.nz;
+        const C* cu = z.coefUz + (long long)at * z.nz;
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if (e < ncell) {
+                const int m = e / z.nz;
+                const int kz = e - m * z.nz;
+                const int s = m * z.ps + kz;
+                const C A = fa[e], X = fa[z.fstride + e], Y = fa[2 * z.fstride + e];
+                const C e1 = ce[kz], u1 = cu[kz];
+                buf[s] = cmul(e1, A);
+                buf[plane + s] = cmul(e1, X);
+                buf[2 * plane + s] = cmul(e1, Y);
+                buf[3 * plane + s] = cmul(u1, A);
+            }
+        }
+        __syncthreads();
+        fft_pencils<T, EPT>(buf, pg, z.zp, tid, NT);
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if (e < ncell) {
+                const int m = e / z.nz;
+                const int s = m * z.ps + (e - m * z.nz);
+                const C gE = buf[s], gX = buf[plane + s], gY = buf[2 * plane + s], gZ = buf[3 * plane + s];
+                if (z.in.wdense) {
+                    for (int p = 0; p < z.in.nPhase; p++) {
+                        const T w = z.in.wdense[p * n + g0 + e];
+                        if (w != T(0)) add_adjoint<T>(cell[q], apc[p * z.nAtom + at], w, a.qc, gE, gX, gY, gZ, dU[q], dP[q]);
+                    }
+                } else if (ph[q] >= 0 && ph[q] < z.in.nPhase) {
+                    add_adjoint<T>(cell[q], apc[ph[q] * z.nAtom + at], wt[q], a.qc, gE, gX, gY, gZ, dU[q], dP[q]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int e = tid + q * NT;
+        if (e < ncell) {
+            const long long g = g0 + e;
+            for (int d = 0; d < 3; d++) {
+                a.dU[d * n + g] = dU[q][d];
+                a.dP[d * n + g] = d < z.in.nStruc ? dP[q][d] : T(0);
+            }
+        }
     }
 }
 

@@ -228,6 +228,31 @@ class Plan:
             return {"P": P, "U": U, "phase": None, "weight": None, "wdense": wdense}
         return {"P": P, "U": U, "phase": phase, "weight": weight if flags.value & 2 else None, "wdense": None}
 
+    def adjoint(self, inputs, grad_I, stream=None):
+        """
+        dL/dP and dL/dU (each 3 * n in the plan precision) for packed inputs and dL/dI, a float64 CUDA
+        tensor of n values laid out like I (fftshifted).  The forward is recomputed on the device.
+        """
+        import torch
+        if self.crystal is None:
+            raise RuntimeError("set_crystal() first")
+        dev = torch.device("cuda", self.device)
+        g = grad_I.reshape(-1)
+        if g.dtype != torch.float64 or g.numel() != self.n or g.device != dev:
+            raise ValueError(f"grad_I: expected {self.n} float64 values on {dev}")
+        g = g.contiguous()
+        dP = torch.empty(3 * self.n, dtype=self.torch_dtype, device=dev)
+        dU = torch.empty(3 * self.n, dtype=self.torch_dtype, device=dev)
+
+        def p(t):
+            return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+        st = ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream)
+        self._check(self.lib.qpd_adjoint_device(self._ctx, p(inputs["P"]), p(inputs["U"]), p(inputs.get("phase")),
+                                                p(inputs.get("weight")), p(inputs.get("wdense")), p(g), p(dP),
+                                                p(dU), st))
+        return dP, dU
+
     def pack_fields(self, P, material, dc, phase_of, ramp_dz, z0=0, u=None, phase=None, region=None,
                     p_scale=1.0, u_scale=1e9, stream=None):
         """
