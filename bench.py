@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving (request loop) leg")
     ap.add_argument("--serving-requests", type=int, default=400)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation (adjoint) leg")
     ap.add_argument("--config", type=int, default=2, choices=(2, 3),
                     help="3: the 4000x4000x68 twin film on one GPU (device-resident, per-pass roofline)")
     ap.add_argument("--validate", action="store_true", help="with --config 3: compare against a float64 plain run")
@@ -320,6 +321,71 @@ def serving_leg(args, torch, device):
     return out
 
 
+def adjoint_leg(args, torch, device, steps=20):
+    """
+    Differentiation workload: 256 x 256 x 64 polar-vortex film, loss sum_q (log10 I - log10 I_target)^2
+    with I_target from the unperturbed field, evaluated at P + N(0, 0.05), u + N(0, 0.001 nm).
+    Times forward + loss + backward (the hand-written adjoint recomputes the forward) in float32 and
+    compares its gradients with the float64 adjoint of the same kernels.
+    """
+    from qpop_diffraction_b200 import Plan, autograd, crystal_from, workloads
+    shape = (256, 256, 64)
+    dev = torch.device("cuda", device)
+    params, inputs = workloads.gpu_snapshot("vortex", shape, seed=5, device=f"cuda:{device}")
+    crystal = crystal_from(params, workloads.config2_crystal(2, (1, 0, 3)))
+    n = params.n
+    g = torch.Generator(device=dev)
+    g.manual_seed(6)
+    dP = torch.randn(3 * n, generator=g, device=dev) * 0.05
+    dU = torch.randn(3 * n, generator=g, device=dev) * 0.001
+    out = {}
+    grads = {}
+    for precision in ("fp32", "fp64"):
+        with Plan(shape, (params.dx, params.dy, params.dz), params.nPhase, 3, precision=precision, device=device) as plan:
+            plan.set_crystal(crystal)
+            dt = plan.torch_dtype
+            base = dict(inputs, P=inputs["P"].to(dt), U=inputs["U"].to(dt))
+            target = plan.run_device(base).clone() if precision == "fp32" else grads["target"]
+            grads["target"] = target
+            P0 = (inputs["P"].reshape(-1) + dP).to(dt).view((3,) + shape)
+            U0 = (inputs["U"].reshape(-1) + dU).to(dt).view((3,) + shape)
+
+            def step():
+                P = P0.clone().requires_grad_(True)
+                U = U0.clone().requires_grad_(True)
+                I = autograd.intensity(plan, P, U, phase=base["phase"], weight=base["weight"])
+                loss = ((torch.log10(I) - torch.log10(target)) ** 2).sum()
+                loss.backward()
+                return loss, P.grad, U.grad
+
+            for _ in range(3):
+                step()
+            k = steps if precision == "fp32" else 3
+            plan.enable_timing(True)
+            torch.cuda.synchronize(dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(k):
+                loss, gP, gU = step()
+            b.record()
+            torch.cuda.synchronize(dev)
+            plan.device_status()
+            st = plan.stage_times()
+            plan.enable_timing(False)
+            grads[precision] = (gP.double(), gU.double())
+            out[precision] = {"ms_per_step": a.elapsed_time(b) / k, "steps": k, "loss": loss.item(),
+                              "adjoint_ms": sum(st[kk][0] for kk in st if kk.startswith("adj")) / k,
+                              "kernels_ms": {kk: v[0] / k for kk, v in st.items()}}
+    (p32, u32), (p64, u64) = grads["fp32"], grads["fp64"]
+    rel = lambda x, y: ((x - y).abs().max() / y.abs().max()).item()
+    cos = lambda x, y: ((x * y).sum() / (x.norm() * y.norm())).item()
+    out.update({"grid": list(shape), "cells": n, "texture": "vortex (seed 5), G=103",
+                "fp32_vs_fp64_grad": {"dP_max_rel": rel(p32, p64), "dU_max_rel": rel(u32, u64),
+                                      "dP_cos": cos(p32, p64), "dU_cos": cos(u32, u64)},
+                "step": "forward + log10 loss + backward (hand-written adjoint, forward recomputed per pass)"})
+    return out
+
+
 def main():
     args = parse()
     from qpop_diffraction_b200 import replicas
@@ -400,6 +466,7 @@ def main():
         p.enable_timing(False)
     ms = replicas.slowest(ms, dev)
     value = replicas.throughput(args.steps * n, ms * 1e-3, world) / 1e9
+    I32 = plans[0].run_device(packed).clone()      # G = 002, for the float32-vs-float64 accuracy
 
     hbm, hbm_src = peaks()
     weight = packed["weight"] is not None
@@ -443,6 +510,7 @@ def main():
 
     # ---------------- float64: the same kernels, fused and plain ----------------
     fp64 = None
+    accuracy = None
     if not args.no_fp64:
         fp64 = {}
         for schedule, k in (("fused", min(args.steps, 10)), ("plain", min(args.steps, 3))):
@@ -459,11 +527,30 @@ def main():
             torch.cuda.synchronize(dev)
             t = a.elapsed_time(b) / k
             fp64[schedule] = {"value": n / (t * 1e-3) / 1e9, "ms_per_step": t, "steps": k}
+            if schedule == "plain":
+                I64 = ps[0].run_device(pk)
+                imax = I64.max()
+                strong = I64 > 1e-6 * imax
+                dlog = (torch.log10(I32) - torch.log10(I64)).abs()
+                accuracy = {"against": "float64 plain schedule (the reference's per-atom loop), G=002, full grid",
+                            "max_abs_over_Imax": ((I32 - I64).abs().max() / imax).item(),
+                            "max_rel_above_1e-6_Imax": ((I32 - I64).abs()[strong] / I64[strong]).max().item(),
+                            "log10_I_max_err_above_1e-6_Imax": dlog[strong].max().item(),
+                            "log10_I_p99_err_all": torch.quantile(dlog.flatten()[::97].float(), 0.99).item(),
+                            "contract": "max |dI|/I_max <= 1e-5, rel <= 1e-3 above 1e-6 I_max"}
+                del I64, strong, dlog
             for p in ps:
                 p.close()
             del pk
         for v in fp64.values():
             v["fp32_speedup"] = v["ms_per_step"] / (ms / args.steps)
+
+    del I32
+    # ---------------- differentiation: forward + backward at 256 x 256 x 64 ----------------
+    adjoint = None
+    if not args.no_adjoint:
+        torch.cuda.empty_cache()
+        adjoint = adjoint_leg(args, torch, local)
 
     # ---------------- serving: Poisson mix of grids over resident snapshots ----------------
     serving = None
@@ -494,7 +581,7 @@ def main():
                        "l2": "no flush: every step reads and writes about 4 GB, far above the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "roofline": roof, "model_roofline": model, "kernels": per_kernel, "gpu_launches": launches,
-            "e2e": e2e, "fp64": fp64, "serving": serving, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "e2e": e2e, "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "serving": serving, "cpu_baseline": cpu, "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

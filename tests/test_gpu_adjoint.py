@@ -133,3 +133,57 @@ def test_adjoint_needs_the_fused_schedule(gpu):
         packed = plan.pack(t(case.oPhase), t(case.oStruc), t(case.u), t(case.region))
         with pytest.raises(ValueError):
             plan.adjoint(packed, torch.ones(plan.n, dtype=torch.float64, device="cuda"))
+
+
+def config5(torch, precision, seed=5):
+    """256 x 256 x 64 polar-vortex film, target from the unperturbed field, P + N(0, 0.05), u + N(0, 0.001 nm)."""
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    shape = (256, 256, 64)
+    params, inputs = workloads.gpu_snapshot("vortex", shape, seed=seed, device="cuda:0")
+    crystal = crystal_from(params, workloads.config2_crystal(2, (1, 0, 3)))
+    plan = Plan(shape, (params.dx, params.dy, params.dz), params.nPhase, 3, precision=precision)
+    plan.set_crystal(crystal)
+    g = torch.Generator(device="cuda:0")
+    g.manual_seed(seed + 1)
+    dt = plan.torch_dtype
+    base = {k: (v.to(dt) if v is not None and v.is_floating_point() else v) for k, v in inputs.items()}
+    target = plan.run_device(base).clone()
+    P = (inputs["P"].reshape(-1) + torch.randn(3 * plan.n, generator=g, device="cuda:0") * 0.05).float()
+    U = (inputs["U"].reshape(-1) + torch.randn(3 * plan.n, generator=g, device="cuda:0") * 0.001).float()
+    packed = dict(base, P=P.to(dt), U=U.to(dt))
+    w = torch.ones(plan.n, dtype=torch.float64, device="cuda:0") if inputs["weight"] is None else inputs["weight"].double()
+    W = torch.stack([(inputs["phase"].long() == p).double() * w for p in range(params.nPhase)]).view((params.nPhase,) + shape)
+    return plan, crystal, packed, target, W
+
+
+def test_config5_full_size_against_complex128_and_finite_differences(gpu):
+    """The 256 x 256 x 64 differentiation workload: float32 adjoint vs complex128 autograd and 64-voxel FD."""
+    torch = gpu
+    plan, crystal, packed, target, W = config5(torch, "fp32")
+    with plan:
+        _, gP, gU = grads_ours(torch, plan, packed, target)
+        _, rP, rU = grads_torch(torch, plan, crystal, packed, target, W)
+    assert rel(gP, rP) <= 2e-3, rel(gP, rP)
+    assert rel(gU, rU) <= 2e-3, rel(gU, rU)
+    del rP, rU
+    torch.cuda.empty_cache()
+    fplan, _, fpacked, _, _ = config5(torch, "fp64")
+    ftarget = target                        # the same loss: only the forward's precision differs
+    rng = np.random.default_rng(64)
+    n = fplan.n
+    fd, ad = [], []
+    with fplan:
+        for name in ("P", "U"):
+            for _ in range(32):
+                comp, cell = int(rng.integers(3)), int(rng.integers(n))
+                h = 1e-4 if name == "P" else 1e-5
+                vals = []
+                for sgn in (1, -1):
+                    x = dict(fpacked)
+                    x[name] = fpacked[name].clone()
+                    x[name][comp * n + cell] += sgn * h
+                    vals.append(tref.log_loss(fplan.run_device(x), ftarget).item())
+                fd.append((vals[0] - vals[1]) / (2 * h))
+                ad.append((gP if name == "P" else gU).reshape(-1)[comp * n + cell].item())
+    fd, ad = np.array(fd), np.array(ad)
+    assert np.abs(fd - ad).max() / np.abs(fd).max() <= 2e-3
