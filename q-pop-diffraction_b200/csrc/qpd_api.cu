@@ -19,6 +19,7 @@
 #include "qpopdiff.h"
 #include "qpd_fast.cuh"
 #include "qpd_fields.cuh"
+#include "qpd_zpfa.cuh"
 #include "qpd_host.h"
 #include "qpd_kernels.cuh"
 
@@ -91,6 +92,13 @@ struct qpd_ctx {
     // QPOP_B200_NBUF (tile buffers of the TMA passes, 2 or 3)
     int knob_z = 0;
     int knob_nbuf = 2;
+    // z stage for nz = 104 and 68: the register-fused prime-factor kernel (zstage_pfa) or the Stockham one.
+    // Default (-1): fused for nz = 68 (69.8 against 89.3 ms at 4000x4000x68), Stockham for nz = 104 (1.81
+    // against 1.84 ms at 512x512x104); QPOP_B200_ZPFA=0 or 1 forces one of them for both lengths.
+    int knob_zpfa = -1;
+    // QPOP_B200_N4000: launch shape of the 4000-point passes (0: 512 threads, 2 buffers; 1: one
+    // buffer, two CTAs per SM; 2: 1024 threads)
+    int knob_n4000 = 0;
 
     // per-kernel timing
     bool timing = false;
@@ -735,10 +743,40 @@ template <typename T> struct Impl {
         return tstop(c, QPD_K_ZSTAGE, st, t0);
     }
 
+    template <int N1, int N2> static int pfa_z_(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
+        using L = ZPfaLayout<T, N1, N2>;
+        constexpr int NT = ZPfa<N1, N2>::NT;
+        a.M = L::M;
+        a.ps = L::PS;
+        const size_t smem = L::bytes(a.in.nPhase * a.nAtom, a.nAtom);
+        if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "z stage tables exceed shared memory");
+        QPD_TRY(set_smem(c, zstage_pfa<T, N1, N2>, smem));
+        int per_sm = 0, sms = 0;
+        QPD_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zstage_pfa<T, N1, N2>, NT, smem));
+        QPD_CU(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        const int64_t ntiles = (a.ncols + L::M - 1) / L::M;
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sms));
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        zstage_pfa<T, N1, N2><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_ZSTAGE, st, t0);
+    }
+
     // Returns QPD_OK and sets *done when an instantiation covers nz.
     static int fast_z(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st, bool* done) {
         *done = true;
         constexpr bool F = sizeof(T) == 4;
+        if constexpr (F) {
+            // single-phase inputs: the register-fused prime-factor z stage
+            if (c->tma && !a.in.wdense && a.nAtom <= 16) {
+                if (a.nz == 104 && c->knob_zpfa == 1 &&
+                    ZPfaLayout<T, 8, 13>::bytes(a.in.nPhase * a.nAtom, a.nAtom) <= max_smem(c))
+                    return pfa_z_<8, 13>(c, a, st);
+                if (a.nz == 68 && c->knob_zpfa != 0 &&
+                    ZPfaLayout<T, 4, 17>::bytes(a.in.nPhase * a.nAtom, a.nAtom) <= max_smem(c))
+                    return pfa_z_<4, 17>(c, a, st);
+            }
+        }
         if (c->tma && ZLayout<T, 128, 8>::bytes(a.in.nPhase * a.nAtom, a.nAtom) <= max_smem(c)) {
             switch (a.nz) {
                 case 32: return smem_z_<32, F ? 32 : 16, F ? 512 : 256, Radix<8, 4>>(c, a, st);
@@ -842,8 +880,17 @@ template <typename T> struct Impl {
                 if constexpr (sizeof(T) == 4) {
                     if (c->tma && a.nz % 2 == 0) {
                         const bool xp = kind == QPD_K_XPASS || (kind == QPD_K_AXIS && a.stride != a.nz);
-                        if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, Radix<8, 4, 5, 5, 5>, 2>(c, a, nouter, kind, st);
-                        return tma_axis_b<4000, 2, 512, 2, EPI, false, Radix<8, 4, 5, 5, 5>, 2>(c, a, nouter, kind, st);
+                        using R4000 = Radix<8, 4, 5, 5, 5>;
+                        if (c->knob_n4000 == 1) {  // one tile buffer: two CTAs per SM
+                            if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 1>(c, a, nouter, kind, st);
+                            return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 1>(c, a, nouter, kind, st);
+                        }
+                        if (c->knob_n4000 == 2) {  // 1024 threads, two tile buffers
+                            if (xp) return tma_axis_b<4000, 2, 1024, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
+                            return tma_axis_b<4000, 2, 1024, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
+                        }
+                        if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
+                        return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
                     }
                 }
                 break;
@@ -1392,6 +1439,8 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     c->tma = !(notma && notma[0] == '1');
     if (const char* k = std::getenv("QPOP_B200_ZCFG")) c->knob_z = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_NBUF")) c->knob_nbuf = std::atoi(k) == 3 ? 3 : 2;
+    if (const char* k = std::getenv("QPOP_B200_ZPFA")) c->knob_zpfa = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_N4000")) c->knob_n4000 = std::atoi(k);
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete c;

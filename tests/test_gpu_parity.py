@@ -204,3 +204,21 @@ def test_planted_signals(gpu):
             analytic.check_phase_and_region_weights(f)
         else:  # float32: voxels above its noise floor
             analytic.check_phase_and_region_weights(f, rtol=1e-5, lit=1e-6)
+
+
+@pytest.mark.parametrize("shape,weights", [((64, 48, 104), "onehot"), ((40, 36, 68), "region"), ((24, 30, 68), "onehot")])
+def test_prime_factor_z_stage_equals_stockham(gpu, monkeypatch, shape, weights):
+    """The register-fused prime-factor z stage (zstage_pfa) and the Stockham one compute the same volume."""
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    from oracle import diffraction_oracle as oracle
+    case = workloads.random_case(shape, seed=sum(shape), nPhase=2, weights=weights, strain=True, hkl=(1, 0, 3))
+    p = case.params
+    out = []
+    for knob in ("0", "1"):
+        monkeypatch.setenv("QPOP_B200_ZPFA", knob)
+        with Plan(case.shape, (p.dx, p.dy, p.dz), p.nPhase, p.nStruc) as plan:
+            plan.set_crystal(crystal_from(p, case.atoms))
+            out.append(plan.run_host(case.oPhase, case.oStruc, case.u, case.region))
+    assert np.abs(out[0] - out[1]).max() / out[0].max() <= 1e-6
+    ref = oracle.diffraction(*case.args())[0]
+    assert_parity(out[1], ref, "fp32")
