@@ -96,8 +96,8 @@ struct qpd_ctx {
     // Default (-1): fused for nz = 68 (69.8 against 89.3 ms at 4000x4000x68), Stockham for nz = 104 (1.81
     // against 1.84 ms at 512x512x104); QPOP_B200_ZPFA=0 or 1 forces one of them for both lengths.
     int knob_zpfa = -1;
-    // QPOP_B200_N4000: launch shape of the 4000-point passes (0: 512 threads, 2 buffers; 1: one
-    // buffer, two CTAs per SM; 2: 1024 threads)
+    // QPOP_B200_N4000: launch shape of the 4000-point passes (0: 512 threads, 2 buffers, out-of-place
+    // stages; 1: one buffer, two CTAs per SM; 2: 1024 threads; 3: in-place stages)
     int knob_n4000 = 0;
 
     // per-kernel timing
@@ -821,7 +821,7 @@ template <typename T> struct Impl {
         return tma_axis_b<N, CZ, NT, VEC, EPI, XP, RAD, 3>(c, a, nouter, kind, st);
     }
 
-    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF>
+    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF, bool OOP = false>
     static int tma_axis_b(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
         constexpr int BOX = tma_rows(N, CZ * (int)sizeof(C));
         a.Cz = CZ;
@@ -830,13 +830,13 @@ template <typename T> struct Impl {
         const int64_t nfields = c->sched_used == QPD_SCHED_FUSED ? 3 * c->ng1 : 2;
         QPD_TRY(field_map(c, &map, const_cast<C*>(a.in), sizeof(T) == 8, a.nz, c->ny, nfields * c->nx, 2 * CZ,
                           XP ? 1 : BOX, XP ? BOX : 1));
-        const size_t smem = sizeof(C) * N * CZ * NBUF + sizeof(C) * N + 128;
+        const size_t smem = sizeof(C) * N * CZ * (NBUF + (OOP ? 1 : 0)) + sizeof(C) * N + 128;
         if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "axis tile exceeds shared memory");
-        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF>, smem));
+        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP>, smem));
         const int64_t grid = nouter * a.nzc;
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
-        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF><<<(unsigned)grid, NT, smem, st>>>(map, a);
+        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP><<<(unsigned)grid, NT, smem, st>>>(map, a);
         return tstop(c, kind, st, t0);
     }
 
@@ -889,8 +889,13 @@ template <typename T> struct Impl {
                             if (xp) return tma_axis_b<4000, 2, 1024, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
                             return tma_axis_b<4000, 2, 1024, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
                         }
-                        if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
-                        return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
+                        if (c->knob_n4000 == 3) {  // in-place stages (registers hold all butterflies of a stage)
+                            if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
+                            return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
+                        }
+                        // out-of-place stages: 3 tiles of 64 KB + twiddles, one barrier per stage, no spills
+                        if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2, true>(c, a, nouter, kind, st);
+                        return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2, true>(c, a, nouter, kind, st);
                     }
                 }
                 break;

@@ -259,8 +259,11 @@ __host__ __device__ constexpr int tma_rows(int N, int row_bytes) {
     return 0;
 }
 
-template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF>
-__global__ void __launch_bounds__(NT, NT <= 512 && N * CZ * NBUF <= 8192 ? 2 : 1) axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
+// OOP: out-of-place Stockham stages through one more tile of shared memory (one barrier per stage,
+// one butterfly in registers at a time); the in-place stages otherwise.
+template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF, bool OOP = false>
+__global__ void __launch_bounds__(NT, NT <= 512 && N * CZ * (NBUF + (OOP ? 1 : 0)) <= 8192 ? 2 : 1)
+    axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
     using C = C_t<T>;
     static_assert(CZ % VEC == 0, "chunk must hold whole vectors");
     constexpr int NO = 1;  // the host builds single-output segments for this kernel
@@ -276,6 +279,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && N * CZ * NBUF <= 8192 ? 2 : 1
     extern __shared__ __align__(128) unsigned char smem_raw[];
     C* bufs = reinterpret_cast<C*>(smem_raw);
     C* tw = bufs + NBUF * TILE;  // twiddles, N values
+    C* scratch = tw + N;         // OOP: the second buffer of the out-of-place stages
     __shared__ __align__(8) uint64_t bar[NBUF];
     const int tid = threadIdx.x;
     const long long outer = blockIdx.x / a.nzc;
@@ -351,7 +355,9 @@ __global__ void __launch_bounds__(NT, NT <= 512 && N * CZ * NBUF <= 8192 ? 2 : 1
                         mbar_wait(&bar[(fl + k) % NBUF], ((fl + k) / NBUF) & 1, nullptr);
                 return;
             }
-            fft_ct<T, N, GE>(buf, tw, tid, RAD{});
+            C* res = buf;
+            if constexpr (OOP) res = fft_oop<T, N, GE>(buf, scratch, tw, tid, RAD{});
+            else fft_ct<T, N, GE>(buf, tw, tid, RAD{});
             const bool mine = seg.ident ? (fi == 0) : (cf != nullptr);
             if (mine) {
 #pragma unroll
@@ -360,7 +366,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && N * CZ * NBUF <= 8192 ? 2 : 1
                     if (GROUPS % NT == 0 || e < GROUPS) {
                         const int k = e / CV;
                         const int c = (e - k * CV) * VEC;
-                        const C* s = buf + k * CZ + c;
+                        const C* s = res + k * CZ + c;
                         if (seg.ident) {
 #pragma unroll
                             for (int w = 0; w < VEC; w++) acc[0][q][w] = cadd(acc[0][q][w], s[w]);

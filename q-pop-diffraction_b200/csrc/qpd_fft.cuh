@@ -308,6 +308,55 @@ __device__ __forceinline__ void fft_ct(C_t<T>* buf, const C_t<T>* __restrict__ t
     if constexpr (sizeof...(Rs) > 0) fft_ct_<T, N, 1, GE, Rs...>(buf, tw, t);
 }
 
+// Out-of-place Stockham: stage s reads one buffer and writes the other, so a thread needs one
+// butterfly in registers at a time and a stage needs a single barrier (its writes go to the buffer
+// the previous stage read, whose reads all finished at that stage's barrier).  Returns the buffer
+// that holds the result: `a` after an even number of stages, `b` after an odd one.
+template <typename T, int N, int NS, int R, class GE>
+__device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>* __restrict__ dst,
+                                          const C_t<T>* __restrict__ tw, int t) {
+    using C = C_t<T>;
+    constexpr int L = N / R;
+    constexpr int NB = GE::COUNT * L;
+    constexpr int BPT = cdiv(NB, GE::NT);
+    constexpr int TSTEP = N / (NS * R);
+#pragma unroll 2
+    for (int q = 0; q < BPT; q++) {
+        const int b = t + q * GE::NT;
+        if (NB % GE::NT == 0 || b < NB) {
+            const int pc = b % GE::COUNT;
+            const int j = b / GE::COUNT;
+            const int k = j % NS;
+            const int pb = GE::base(pc);
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = src[pb + (j + r * L) * GE::ES];
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) v[r] = cmul(v[r], tw[r * k * TSTEP]);
+            }
+            Dft<R, C>::run(v);
+            const int ob = pb + ((j / NS) * NS * R + k) * GE::ES;
+#pragma unroll
+            for (int r = 0; r < R; r++) dst[ob + r * NS * GE::ES] = v[r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int N, int NS, class GE, int R, int... Rest>
+__device__ __forceinline__ C_t<T>* fft_oop_(C_t<T>* a, C_t<T>* b, const C_t<T>* __restrict__ tw, int t) {
+    stage_oop<T, N, NS, R, GE>(a, b, tw, t);
+    if constexpr (sizeof...(Rest) > 0) return fft_oop_<T, N, NS * R, GE, Rest...>(b, a, tw, t);
+    else return b;
+}
+
+template <typename T, int N, class GE, int... Rs>
+__device__ __forceinline__ C_t<T>* fft_oop(C_t<T>* a, C_t<T>* b, const C_t<T>* __restrict__ tw, int t, Radix<Rs...>) {
+    if constexpr (sizeof...(Rs) > 0) return fft_oop_<T, N, 1, GE, Rs...>(a, b, tw, t);
+    else return a;
+}
+
 // ---------------------------------------------------------------------------------------
 // Prime-factor (Good-Thomas) FFT for N = N1 N2 with gcd(N1, N2) = 1: a 2-D DFT without twiddle
 // factors.  Input x[n] is read as A0[n1][n2] = x[(N2 n1 + N1 n2) mod N]; stage A transforms over
