@@ -83,6 +83,8 @@ struct qpd_ctx {
     size_t hring_bytes = 0;
     cudaEvent_t ring_ev[3] = {nullptr, nullptr, nullptr};
     bool ring_busy[3] = {false, false, false};
+    static constexpr int kChunkEv = 8;
+    cudaEvent_t chunk_ev[kChunkEv] = {};
     bool tma = true;  // TMA-fed kernels where the layout allows (QPOP_B200_NO_TMA=1 disables)
 
     // compile-time specialised kernels where an instantiation covers the axis (QPOP_B200_GENERIC=1 disables)
@@ -96,9 +98,13 @@ struct qpd_ctx {
     // Default (-1): fused for nz = 68 (69.8 against 89.3 ms at 4000x4000x68), Stockham for nz = 104 (1.81
     // against 1.84 ms at 512x512x104); QPOP_B200_ZPFA=0 or 1 forces one of them for both lengths.
     int knob_zpfa = -1;
-    // QPOP_B200_N4000: launch shape of the 4000-point passes (0: 512 threads, 2 buffers, out-of-place
-    // stages; 1: one buffer, two CTAs per SM; 2: 1024 threads; 3: in-place stages)
+    // QPOP_B200_N4000: launch shape of the 4000-point passes (0: out-of-place stages, 1024 threads for y
+    // and 512 for x; 1: one buffer, two CTAs per SM; 2: 1024 threads in place; 3: 512 threads in place;
+    // 4: 1024 threads out of place for both)
     int knob_n4000 = 0;
+    // QPOP_B200_OOP=0: in-place stages for the 256- and 512-point TMA passes (out-of-place measured
+    // 1.080 against 1.104 ms for the y pass at 512x512x104)
+    int knob_oop = 1;
 
     // per-kernel timing
     bool timing = false;
@@ -817,6 +823,9 @@ template <typename T> struct Impl {
 
     template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD>
     static int tma_axis_(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+        if constexpr (sizeof(T) == 4 && (N == 512 || N == 256)) {
+            if (c->knob_oop == 1) return tma_axis_b<N, CZ, NT, VEC, EPI, XP, RAD, 2, true>(c, a, nouter, kind, st);
+        }
         if (c->knob_nbuf == 2) return tma_axis_b<N, CZ, NT, VEC, EPI, XP, RAD, 2>(c, a, nouter, kind, st);
         return tma_axis_b<N, CZ, NT, VEC, EPI, XP, RAD, 3>(c, a, nouter, kind, st);
     }
@@ -889,13 +898,19 @@ template <typename T> struct Impl {
                             if (xp) return tma_axis_b<4000, 2, 1024, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
                             return tma_axis_b<4000, 2, 1024, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
                         }
+                        if (c->knob_n4000 == 4) {  // 1024 threads, out-of-place stages
+                            if (xp) return tma_axis_b<4000, 2, 1024, 2, EPI, true, R4000, 2, true>(c, a, nouter, kind, st);
+                            return tma_axis_b<4000, 2, 1024, 2, EPI, false, R4000, 2, true>(c, a, nouter, kind, st);
+                        }
                         if (c->knob_n4000 == 3) {  // in-place stages (registers hold all butterflies of a stage)
                             if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
                             return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
                         }
-                        // out-of-place stages: 3 tiles of 64 KB + twiddles, one barrier per stage, no spills
+                        // out-of-place stages: 3 tiles of 64 KB + twiddles, one barrier per stage; measured at
+                        // 4000x4000x68: y pass 103.0 ms with 1024 threads (109.8 with 512), x pass 55.6 ms with
+                        // 512 (59.0 with 1024)
                         if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2, true>(c, a, nouter, kind, st);
-                        return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2, true>(c, a, nouter, kind, st);
+                        return tma_axis_b<4000, 2, 1024, 2, EPI, false, R4000, 2, true>(c, a, nouter, kind, st);
                     }
                 }
                 break;
@@ -1184,13 +1199,22 @@ template <typename T> struct Impl {
             if (!e) QPD_CU(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         const int64_t C = std::min<int64_t>(n, (int64_t)1 << 21);  // cells per chunk
         constexpr int NSLOT = 3;
-        // Chunks are split between two routes that run at the same time: the host workers pack a
-        // share of them (fewer bytes on the link, host memory bandwidth spent), the others go over
-        // the link as float64 and pack_kernel packs them on the device.
-        double share = 0.8;  // measured best on a 16-core host with pinned inputs (37.9 ms against 50.7 all-device)
+        // Chunks take one of two routes that run at the same time: the host workers pack a chunk
+        // (fewer bytes on the link, host memory bandwidth spent) or it crosses the link as float64
+        // and pack_kernel packs it on the device.  The split balances itself: a chunk goes the device
+        // way whenever no chunk waits on the copy engine, so the link never idles while
+        // the host packs, and a slow host packs fewer chunks (QPOP_B200_ROUTE_DEPTH sets that queue
+        // depth, default 1).  QPOP_B200_HOST_SHARE fixes the share
+        // of host-packed chunks instead (0: all device, 1: all host).
+        double share = -1.0;
         if (const char* e = std::getenv("QPOP_B200_HOST_SHARE")) share = std::min(1.0, std::max(0.0, std::atof(e)));
+        int depth = 1;  // device route while fewer than `depth` chunks wait on the copy engine
+        if (const char* e = std::getenv("QPOP_B200_ROUTE_DEPTH")) depth = std::max(1, std::atoi(e));
         const int NPL = NS + 3 + NP + (region ? 1 : 0);
-        if (share < 1.0) QPD_TRY(dev_reserve(c, c->stage, sizeof(double) * NPL * C, "float64 staging"));
+        constexpr int NSTAGE = 2;  // device-route staging slots
+        if (share < 1.0) QPD_TRY(dev_reserve(c, c->stage, sizeof(double) * NPL * C * NSTAGE, "float64 staging"));
+        for (auto& e : c->chunk_ev)
+            if (!e) QPD_CU(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         QPD_TRY(dev_reserve(c, c->flags, 256, "flags"));
         uint32_t* dflags = static_cast<uint32_t*>(c->flags.p);
         double* sg = static_cast<double*>(c->stage.p);
@@ -1211,16 +1235,34 @@ template <typename T> struct Impl {
                 for (bool& b : c->ring_busy) b = false;
             }
             uint32_t flags = 0;
-            int64_t hosted = 0;
+            int64_t hosted = 0, staged = 0;
+            // completion events of the chunks in flight, oldest first (a ring of kChunkEv)
+            int64_t ev_head = 0, ev_tail = 0;
+            auto pending = [&]() {
+                while (ev_head < ev_tail && cudaEventQuery(c->chunk_ev[ev_head % qpd_ctx::kChunkEv]) == cudaSuccess) ev_head++;
+                return ev_tail - ev_head;
+            };
+            auto record = [&]() -> int {
+                if (ev_tail - ev_head == qpd_ctx::kChunkEv) {  // ring full: wait for the oldest
+                    QPD_CU(c, cudaEventSynchronize(c->chunk_ev[ev_head % qpd_ctx::kChunkEv]));
+                    ev_head++;
+                }
+                QPD_CU(c, cudaEventRecord(c->chunk_ev[ev_tail % qpd_ctx::kChunkEv], st));
+                ev_tail++;
+                return QPD_OK;
+            };
             for (int64_t g0 = 0, i = 0; g0 < n; g0 += C, i++) {
                 const int64_t cnt = std::min(C, n - g0);
-                if ((int64_t)((i + 1) * share) == (int64_t)(i * share)) {  // device route
+                const bool device_route = share >= 0.0 ? (int64_t)((i + 1) * share) == (int64_t)(i * share)
+                                                        : pending() < depth;
+                if (device_route) {
                     const double* ost[3] = {nullptr, nullptr, nullptr};
                     const double* uu[3];
                     const double* oph[kMaxPhases];
+                    double* slot = sg + (size_t)(staged++ % NSTAGE) * NPL * C;
                     int pl = 0;
                     auto put = [&](const double* src, const double** dst) -> int {
-                        double* d = sg + (size_t)(pl++) * C;
+                        double* d = slot + (size_t)(pl++) * C;
                         QPD_CU(c, cudaMemcpyAsync(d, src + g0, sizeof(double) * cnt, cudaMemcpyHostToDevice, st));
                         *dst = d;
                         return QPD_OK;
@@ -1231,7 +1273,8 @@ template <typename T> struct Impl {
                     const double* rg = nullptr;
                     if (region) QPD_TRY(put(region, &rg));
                     QPD_TRY(pack(c, g0, cnt, ost, uu, oph, rg, P, U, ph, W, dense ? WD : nullptr, dflags, st));
-                    continue;  // the next device-route chunk's copies follow this pack in stream order
+                    QPD_TRY(record());  // the staging slot is reused two device chunks later, after this pack in stream order
+                    continue;
                 }
                 const int s = (int)(hosted++ % NSLOT);
                 if (c->ring_busy[s]) QPD_CU(c, cudaEventSynchronize(c->ring_ev[s]));
@@ -1262,6 +1305,7 @@ template <typename T> struct Impl {
                 }
                 QPD_CU(c, cudaEventRecord(c->ring_ev[s], st));
                 c->ring_busy[s] = true;
+                QPD_TRY(record());
             }
             uint32_t df = 0;
             QPD_CU(c, cudaMemcpyAsync(&df, dflags, sizeof df, cudaMemcpyDeviceToHost, st));
@@ -1446,6 +1490,7 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     if (const char* k = std::getenv("QPOP_B200_NBUF")) c->knob_nbuf = std::atoi(k) == 3 ? 3 : 2;
     if (const char* k = std::getenv("QPOP_B200_ZPFA")) c->knob_zpfa = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_N4000")) c->knob_n4000 = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_OOP")) c->knob_oop = std::atoi(k);
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete c;
@@ -1474,6 +1519,8 @@ int qpd_destroy(qpd_ctx* c) {
     c->workers.reset();
     if (c->hring) cudaFreeHost(c->hring);
     for (cudaEvent_t e : c->ring_ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->chunk_ev)
         if (e) cudaEventDestroy(e);
     for (auto& r : c->recs) {
         cudaEventDestroy(r.a);

@@ -262,7 +262,7 @@ __host__ __device__ constexpr int tma_rows(int N, int row_bytes) {
 // OOP: out-of-place Stockham stages through one more tile of shared memory (one barrier per stage,
 // one butterfly in registers at a time); the in-place stages otherwise.
 template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF, bool OOP = false>
-__global__ void __launch_bounds__(NT, NT <= 512 && N * CZ * (NBUF + (OOP ? 1 : 0)) <= 8192 ? 2 : 1)
+__global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (NBUF + (OOP ? 1 : 0)) + N) <= 110 * 1024 ? 2 : 1)
     axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
     using C = C_t<T>;
     static_assert(CZ % VEC == 0, "chunk must hold whole vectors");
