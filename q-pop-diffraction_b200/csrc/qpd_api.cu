@@ -98,9 +98,9 @@ struct qpd_ctx {
     // Default (-1): fused for nz = 68 (69.8 against 89.3 ms at 4000x4000x68), Stockham for nz = 104 (1.81
     // against 1.84 ms at 512x512x104); QPOP_B200_ZPFA=0 or 1 forces one of them for both lengths.
     int knob_zpfa = -1;
-    // QPOP_B200_N4000: launch shape of the 4000-point passes (0: out-of-place stages, 1024 threads for y
-    // and 512 for x; 1: one buffer, two CTAs per SM; 2: 1024 threads in place; 3: 512 threads in place;
-    // 4: 1024 threads out of place for both)
+    // QPOP_B200_N4000: launch shape of the 4000-point passes (0: 512 threads, out-of-place swizzled
+    // stages; 1: one buffer, two CTAs per SM; 2: 1024 threads in place; 3: 512 threads in place;
+    // 4: 1024 threads out of place)
     int knob_n4000 = 0;
     // QPOP_B200_OOP=0: in-place stages for the 256- and 512-point TMA passes (out-of-place measured
     // 1.080 against 1.104 ms for the y pass at 512x512x104)
@@ -906,11 +906,11 @@ template <typename T> struct Impl {
                             if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2>(c, a, nouter, kind, st);
                             return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2>(c, a, nouter, kind, st);
                         }
-                        // out-of-place stages: 3 tiles of 64 KB + twiddles, one barrier per stage; measured at
-                        // 4000x4000x68: y pass 103.0 ms with 1024 threads (109.8 with 512), x pass 55.6 ms with
-                        // 512 (59.0 with 1024)
+                        // out-of-place swizzled stages: 3 tiles of 64 KB + twiddles, one barrier per stage;
+                        // measured at 4000x4000x68: y pass 98.2 ms with 512 threads (108.8 with 1024), x pass
+                        // 53.2 ms
                         if (xp) return tma_axis_b<4000, 2, 512, 2, EPI, true, R4000, 2, true>(c, a, nouter, kind, st);
-                        return tma_axis_b<4000, 2, 1024, 2, EPI, false, R4000, 2, true>(c, a, nouter, kind, st);
+                        return tma_axis_b<4000, 2, 512, 2, EPI, false, R4000, 2, true>(c, a, nouter, kind, st);
                     }
                 }
                 break;

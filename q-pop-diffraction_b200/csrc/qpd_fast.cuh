@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                     if (GROUPS % NT == 0 || e < GROUPS) {
                         const int k = e / CV;
                         const int c = (e - k * CV) * VEC;
-                        const C* s = res + k * CZ + c;
+                        const C* s = res + (OOP ? oop_swz(k) : k) * CZ + c;
                         if (seg.ident) {
 #pragma unroll
                             for (int w = 0; w < VEC; w++) acc[0][q][w] = cadd(acc[0][q][w], s[w]);

@@ -312,9 +312,18 @@ __device__ __forceinline__ void fft_ct(C_t<T>* buf, const C_t<T>* __restrict__ t
 // butterfly in registers at a time and a stage needs a single barrier (its writes go to the buffer
 // the previous stage read, whose reads all finished at that stage's barrier).  Returns the buffer
 // that holds the result: `a` after an even number of stages, `b` after an odd one.
-template <typename T, int N, int NS, int R, class GE>
+//
+// Every buffer a stage writes holds element i at position oop_swz(i): the first stage writes
+// elements R apart from neighbouring threads, which would put them on the same bank; the XOR of
+// the element's block index into its low 3 bits spreads them.  It permutes within aligned blocks of
+// 8 (N % 8 == 0), so contiguous reads stay conflict-free.  The input of the first stage (the loaded
+// tile) is in natural order.
+__device__ __forceinline__ int oop_swz(int i) { return i ^ ((i >> 3) & 7); }
+
+template <typename T, int N, int NS, int R, class GE, bool SWZ_IN>
 __device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>* __restrict__ dst,
                                           const C_t<T>* __restrict__ tw, int t) {
+    static_assert(N % 8 == 0, "the stage swizzle permutes blocks of 8");
     using C = C_t<T>;
     constexpr int L = N / R;
     constexpr int NB = GE::COUNT * L;
@@ -330,15 +339,18 @@ __device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>
             const int pb = GE::base(pc);
             C v[R];
 #pragma unroll
-            for (int r = 0; r < R; r++) v[r] = src[pb + (j + r * L) * GE::ES];
+            for (int r = 0; r < R; r++) {
+                const int i = j + r * L;
+                v[r] = src[pb + (SWZ_IN ? oop_swz(i) : i) * GE::ES];
+            }
             if (NS > 1) {
 #pragma unroll
                 for (int r = 1; r < R; r++) v[r] = cmul(v[r], tw[r * k * TSTEP]);
             }
             Dft<R, C>::run(v);
-            const int ob = pb + ((j / NS) * NS * R + k) * GE::ES;
+            const int ob = (j / NS) * NS * R + k;
 #pragma unroll
-            for (int r = 0; r < R; r++) dst[ob + r * NS * GE::ES] = v[r];
+            for (int r = 0; r < R; r++) dst[pb + oop_swz(ob + r * NS) * GE::ES] = v[r];
         }
     }
     __syncthreads();
@@ -346,15 +358,16 @@ __device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>
 
 template <typename T, int N, int NS, class GE, int R, int... Rest>
 __device__ __forceinline__ C_t<T>* fft_oop_(C_t<T>* a, C_t<T>* b, const C_t<T>* __restrict__ tw, int t) {
-    stage_oop<T, N, NS, R, GE>(a, b, tw, t);
+    stage_oop<T, N, NS, R, GE, (NS > 1)>(a, b, tw, t);
     if constexpr (sizeof...(Rest) > 0) return fft_oop_<T, N, NS * R, GE, Rest...>(b, a, tw, t);
     else return b;
 }
 
+// Result element k of pencil p sits at oop_swz(k) (see stage_oop).
 template <typename T, int N, class GE, int... Rs>
 __device__ __forceinline__ C_t<T>* fft_oop(C_t<T>* a, C_t<T>* b, const C_t<T>* __restrict__ tw, int t, Radix<Rs...>) {
-    if constexpr (sizeof...(Rs) > 0) return fft_oop_<T, N, 1, GE, Rs...>(a, b, tw, t);
-    else return a;
+    static_assert(sizeof...(Rs) > 0, "at least one stage");
+    return fft_oop_<T, N, 1, GE, Rs...>(a, b, tw, t);
 }
 
 // ---------------------------------------------------------------------------------------
