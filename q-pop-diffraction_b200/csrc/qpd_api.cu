@@ -102,6 +102,10 @@ struct qpd_ctx {
     // stages; 1: one buffer, two CTAs per SM; 2: 1024 threads in place; 3: 512 threads in place;
     // 4: 1024 threads out of place)
     int knob_n4000 = 0;
+    // QPOP_B200_YFAST=0: keep the z-fastest field layout at 4000 x 4000 x 68 (the y-fastest route writes
+    // the z stage's fields with y fastest so the 4000-point y transforms read contiguous pencils)
+    int knob_yfast = 1;
+    int knob_bulk_nt = 256;  // QPOP_B200_BULK_NT: threads of the bulk y pass (256: 72.8 ms, 512: 80.9 ms)
     // QPOP_B200_OOP=0: in-place stages for the 256- and 512-point TMA passes (out-of-place measured
     // 1.080 against 1.104 ms for the y pass at 512x512x104)
     int knob_oop = 1;
@@ -830,23 +834,45 @@ template <typename T> struct Impl {
         return tma_axis_b<N, CZ, NT, VEC, EPI, XP, RAD, 3>(c, a, nouter, kind, st);
     }
 
-    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF, bool OOP = false>
+    // YZ: the x pass over fields laid out (x, k_z, y): a.nz is then the y extent and nouter the k_z extent
+    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF, bool OOP = false, bool YZ = false>
     static int tma_axis_b(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
         constexpr int BOX = tma_rows(N, CZ * (int)sizeof(C));
         a.Cz = CZ;
         a.nzc = (a.nz + CZ - 1) / CZ;
+        a.nouter = (int)nouter;
         CUtensorMap map;
         const int64_t nfields = c->sched_used == QPD_SCHED_FUSED ? 3 * c->ng1 : 2;
-        QPD_TRY(field_map(c, &map, const_cast<C*>(a.in), sizeof(T) == 8, a.nz, c->ny, nfields * c->nx, 2 * CZ,
-                          XP ? 1 : BOX, XP ? BOX : 1));
+        QPD_TRY(field_map(c, &map, const_cast<C*>(a.in), sizeof(T) == 8, a.nz, YZ ? c->nz : c->ny, nfields * c->nx,
+                          2 * CZ, XP ? 1 : BOX, XP ? BOX : 1));
         const size_t smem = sizeof(C) * N * CZ * (NBUF + (OOP ? 1 : 0)) + sizeof(C) * N + 128;
         if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "axis tile exceeds shared memory");
-        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP>, smem));
+        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ>, smem));
         const int64_t grid = nouter * a.nzc;
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
-        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP><<<(unsigned)grid, NT, smem, st>>>(map, a);
+        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ><<<(unsigned)grid, NT, smem, st>>>(map, a);
         return tstop(c, kind, st, t0);
+    }
+
+    // y pass over fields laid out (x, k_z, y): one contiguous pencil per CTA (axis_bulk)
+    template <int N, int NT, class RAD> static int bulk_axis_(qpd_ctx* c, AxisArgs<T>& a, cudaStream_t st) {
+        const size_t smem = sizeof(C) * (3 * N + (N + 63) / 64 + 64) + 128;
+        if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "axis pencils exceed shared memory");
+        QPD_TRY(set_smem(c, axis_bulk<T, N, NT, RAD>, smem));
+        const int64_t grid = c->nx * c->nz;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        axis_bulk<T, N, NT, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_YPASS, st, t0);
+    }
+
+    // The 4000 x 4000 x 68 route: fused z stage writing y-fastest fields, bulk y pass, swapped x pass.
+    static bool yfast_ok(qpd_ctx* c, const Inputs<T>& in) {
+        if constexpr (sizeof(T) != 4) return false;
+        return c->knob_yfast && c->fast && c->tma && c->knob_zpfa != 0 && !in.wdense && c->nAtom <= 16 &&
+               c->nx == 4000 && c->ny == 4000 && c->nz == 68 &&
+               ZPfaLayout<T, 4, 17>::bytes(in.nPhase * c->nAtom, c->nAtom) <= max_smem(c);
     }
 
     // float: z chunks of 8 complex64 (64-byte rows), 16-byte accesses when nz is even;
@@ -1025,13 +1051,21 @@ template <typename T> struct Impl {
         return run_adj_z(c, az, st);
     }
 
-    static int forward_zy(qpd_ctx* c, const Inputs<T>& in, cudaStream_t st) {
+    static int forward_zy(qpd_ctx* c, const Inputs<T>& in, cudaStream_t st, bool yfast = false) {
         C* F = static_cast<C*>(c->fields.p);
         const int64_t n = c->n;
         {
             ZArgs<T> z = zargs(c, in);
             bool done = false;
-            if (c->fast) QPD_TRY(fast_z(c, z, st, &done));
+            if constexpr (sizeof(T) == 4) {
+                if (yfast) {
+                    z.yfast = 1;
+                    z.ny = c->ny;
+                    QPD_TRY((pfa_z_<4, 17>(c, z, st)));
+                    done = true;
+                }
+            }
+            if (!done && c->fast) QPD_TRY(fast_z(c, z, st, &done));
             if (!done) QPD_TRY(run_z(c, z, st));
 
             AxisArgs<T> y;
@@ -1049,6 +1083,12 @@ template <typename T> struct Impl {
             y.nx = c->nx;
             y.ny = c->ny;
             y.status = static_cast<int*>(c->status.p);
+            if (yfast) {
+                if constexpr (sizeof(T) == 4) {
+                    if (c->knob_bulk_nt == 512) return bulk_axis_<4000, 512, Radix<8, 4, 5, 5, 5>>(c, y, st);
+                    return bulk_axis_<4000, 256, Radix<8, 4, 5, 5, 5>>(c, y, st);
+                }
+            }
             done = false;
             if (c->fast) QPD_TRY(fast_axis<false>(c, y, c->nx, QPD_K_YPASS, st, &done));
             if (!done) QPD_TRY(run_axis<0>(c, y, c->nx, QPD_K_YPASS, st));
@@ -1060,9 +1100,17 @@ template <typename T> struct Impl {
         C* F = static_cast<C*>(c->fields.p);
         const int64_t n = c->n;
         if (c->sched_used == QPD_SCHED_FUSED) {
-            QPD_TRY(forward_zy(c, in, st));
+            const bool yfast = yfast_ok(c, in);
+            QPD_TRY(forward_zy(c, in, st, yfast));
             AxisArgs<T> x = xargs(c);
             x.I = I;
+            if constexpr (sizeof(T) == 4) {
+                if (yfast) {
+                    x.nz = (int)c->ny;  // the contiguous axis of the y-fastest fields
+                    return tma_axis_b<4000, 2, 512, 2, true, true, Radix<8, 4, 5, 5, 5>, 2, true, true>(c, x, c->nz,
+                                                                                                    QPD_K_XPASS, st);
+                }
+            }
             bool done = false;
             if (c->fast) QPD_TRY(fast_axis<true>(c, x, c->ny, QPD_K_XPASS, st, &done));
             if (done) return QPD_OK;
@@ -1491,6 +1539,8 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     if (const char* k = std::getenv("QPOP_B200_ZPFA")) c->knob_zpfa = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_N4000")) c->knob_n4000 = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_OOP")) c->knob_oop = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_YFAST")) c->knob_yfast = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_BULK_NT")) c->knob_bulk_nt = std::atoi(k) == 512 ? 512 : 256;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete c;

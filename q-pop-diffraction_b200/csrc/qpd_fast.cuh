@@ -261,7 +261,10 @@ __host__ __device__ constexpr int tma_rows(int N, int row_bytes) {
 
 // OOP: out-of-place Stockham stages through one more tile of shared memory (one barrier per stage,
 // one butterfly in registers at a time); the in-place stages otherwise.
-template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF, bool OOP = false>
+// YZ (x pass with EPI only): the fields are laid out (x, k_z, y) with y fastest, so a tile holds CZ
+// values of k_y at one k_z; CTAs take k_z fastest, so the CTAs writing neighbouring z of I run together.
+template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF, bool OOP = false,
+          bool YZ = false>
 __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (NBUF + (OOP ? 1 : 0)) + N) <= 110 * 1024 ? 2 : 1)
     axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
     using C = C_t<T>;
@@ -281,9 +284,10 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
     C* tw = bufs + NBUF * TILE;  // twiddles, N values
     C* scratch = tw + N;         // OOP: the second buffer of the out-of-place stages
     __shared__ __align__(8) uint64_t bar[NBUF];
+    static_assert(!YZ || (EPI && XPASS), "the y-fastest layout is read by the x pass only");
     const int tid = threadIdx.x;
-    const long long outer = blockIdx.x / a.nzc;
-    const int z0 = (int)(blockIdx.x % a.nzc) * CZ;
+    const long long outer = YZ ? blockIdx.x % a.nouter : blockIdx.x / a.nzc;
+    const int z0 = (int)(YZ ? blockIdx.x / a.nouter : blockIdx.x % a.nzc) * CZ;
     const int cz = min(CZ, a.nz - z0);
     const long long base = outer * a.ostride + z0;
     for (int i = tid; i < N; i += NT) tw[i] = static_cast<const C*>(a.ap.tw)[i];
@@ -356,7 +360,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                 return;
             }
             C* res = buf;
-            if constexpr (OOP) res = fft_oop<T, N, GE>(buf, scratch, tw, tid, RAD{});
+            if constexpr (OOP) res = fft_oop<T, N, GE>(buf, scratch, TwFull<C>{tw}, tid, RAD{});
             else fft_ct<T, N, GE>(buf, tw, tid, RAD{});
             const bool mine = seg.ident ? (fi == 0) : (cf != nullptr);
             if (mine) {
@@ -383,7 +387,33 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                 issue(fl + NBUF, b);
             }
         }
-        if (EPI) {
+        if constexpr (EPI && YZ) {
+            // outer = k_z, z0 + c + w = k_y; I is (x, y, z) with z fastest
+            const long long nzr = a.nouter;
+            const long long kz = outer;
+            const long long sz = (kz + nzr / 2) % nzr;
+            const double szv = a.S[2][kz];
+#pragma unroll
+            for (int q = 0; q < EP; q++) {
+                const int e = tid + q * NT;
+                if (GROUPS % NT == 0 || e < GROUPS) {
+                    const int kx = e / CV;
+                    const int c = (e - kx * CV) * VEC;
+                    const double sxz = a.S[0][kx] * szv;
+                    const long long row = (kx + a.nx / 2) % a.nx * a.ny;
+#pragma unroll
+                    for (int w = 0; w < VEC; w++) {
+                        const int ky = z0 + c + w;
+                        if (c + w < cz) {
+                            const double S = sxz * a.S[1][ky];
+                            const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
+                            const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
+                            a.I[(row + (ky + a.ny / 2) % a.ny) * nzr + sz] = v;
+                        }
+                    }
+                }
+            }
+        } else if (EPI) {
             const long long ky = outer;
             const long long sy = (ky + a.ny / 2) % a.ny;
             const double syv = a.S[1][ky];
@@ -436,6 +466,105 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                     }
                 }
             }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// y pass over fields laid out (x, k_z, y), y fastest: one pencil (x, k_z) of N contiguous values per
+// CTA.  Each input field's pencil arrives by 1-D bulk copies in one of two buffers while the
+// previous field is transformed (out-of-place swizzled stages through a third buffer, twiddles from
+// a two-level table) and folded into this thread's accumulators; the outputs go back in place, in
+// the same layout (the CTA owns its pencil in every field).  Three pencils of shared memory, so two
+// CTAs share an SM even for N = 4000.
+// ---------------------------------------------------------------------------------------
+template <typename T, int N, int NT, class RAD>
+__global__ void __launch_bounds__(NT, 2) axis_bulk(AxisArgs<T> a) {
+    using C = C_t<T>;
+    constexpr int NBUF = 2, PIECES = 4;
+    constexpr int EP = cdiv(N, NT);
+    constexpr uint32_t BYTES = N * sizeof(C);
+    static_assert(BYTES % (16 * PIECES) == 0 && N % PIECES == 0, "bulk copies of 16-byte multiples");
+    constexpr int NHI = (N + 63) / 64;
+    using GE = Geo<1, 1, 0, 0, 1, NT>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    C* bufs = reinterpret_cast<C*>(smem_raw);
+    C* scratch = bufs + NBUF * N;
+    C* thi = scratch + N;
+    C* tlo = thi + NHI;
+    __shared__ __align__(8) uint64_t bar[NBUF];
+    const int tid = threadIdx.x;
+    const long long pencil = blockIdx.x;  // x nz + k_z; its values start at pencil * N in every field
+    const C* twg = static_cast<const C*>(a.ap.tw);
+    for (int i = tid; i < NHI; i += NT) thi[i] = twg[64 * i];
+    for (int i = tid; i < 64; i += NT) tlo[i] = twg[i];
+    int total = 0;
+    for (int sg = 0; sg < a.nseg; sg++) total += a.segs[sg].nin;
+    auto field_of = [&](int fl) {
+        for (int sg = 0; sg < a.nseg; sg++) {
+            const int k = a.segs[sg].nin;
+            if (fl < k) return a.segs[sg].in[fl];
+            fl -= k;
+        }
+        return 0;
+    };
+    auto issue = [&](int fl, int b) {
+        const C* src = a.in + (long long)field_of(fl) * a.fstride + pencil * N;
+        C* dst = bufs + b * N;
+        mbar_expect_tx(&bar[b], BYTES);
+#pragma unroll
+        for (int k = 0; k < PIECES; k++) bulk_load(dst + k * (N / PIECES), src + k * (N / PIECES), BYTES / PIECES, &bar[b]);
+    };
+    if (smem_u32(smem_raw) % 16 != 0 || reinterpret_cast<uintptr_t>(a.in) % 16 != 0 ||
+        (a.fstride * sizeof(C)) % 16 != 0) {  // bulk copies need 16-byte aligned addresses: refuse, do not load
+        if (tid == 0) atomicExch(a.status, QPD_DEVERR_ALIGN);
+        return;
+    }
+    if (tid == 0) {
+        for (int b = 0; b < NBUF; b++) mbar_init(&bar[b], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int b = 0; b < NBUF && b < total; b++) issue(b, b);
+    const TwTwoLevel<C> tw{thi, tlo};
+
+    int fl = 0;
+    for (int sg = 0; sg < a.nseg; sg++) {
+        const Segment<T>& seg = a.segs[sg];
+        C acc[EP];
+#pragma unroll
+        for (int q = 0; q < EP; q++) acc[q] = cmake<C>(0, 0);
+        for (int fi = 0; fi < seg.nin; fi++, fl++) {
+            const int b = fl % NBUF;
+            C* buf = bufs + b * N;
+            const C* cf = seg.coef[0][fi];
+            const bool ok = mbar_wait(&bar[b], (fl / NBUF) & 1, a.status);
+            if (!__syncthreads_and(ok)) {
+                if (tid == 0)
+                    for (int k = 1; k < NBUF && fl + k < total; k++)
+                        mbar_wait(&bar[(fl + k) % NBUF], ((fl + k) / NBUF) & 1, nullptr);
+                return;
+            }
+            const C* res = fft_oop<T, N, GE>(buf, scratch, tw, tid, RAD{});
+            if (cf) {  // coefficients read after the transform: fewer live registers
+#pragma unroll
+                for (int q = 0; q < EP; q++) {
+                    const int e = tid + q * NT;
+                    if (N % NT == 0 || e < N) cfma(acc[q], cf[e], res[oop_swz(e)]);
+                }
+            }
+            __syncthreads();  // buffer b and the scratch buffer are free again
+            if (tid == 0 && fl + NBUF < total) {
+                fence_proxy_async();
+                issue(fl + NBUF, b);
+            }
+        }
+        C* dst = a.out + (long long)seg.out[0] * a.fstride + pencil * N;
+#pragma unroll
+        for (int q = 0; q < EP; q++) {
+            const int e = tid + q * NT;
+            if (N % NT == 0 || e < N) dst[e] = acc[q];
         }
     }
 }

@@ -320,9 +320,21 @@ __device__ __forceinline__ void fft_ct(C_t<T>* buf, const C_t<T>* __restrict__ t
 // tile) is in natural order.
 __device__ __forceinline__ int oop_swz(int i) { return i ^ ((i >> 3) & 7); }
 
-template <typename T, int N, int NS, int R, class GE, bool SWZ_IN>
-__device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>* __restrict__ dst,
-                                          const C_t<T>* __restrict__ tw, int t) {
+// Twiddle exp(-2 pi i m / N): from a full table, or as the product of a coarse and a fine table
+// (exp(-2 pi i 64 (m >> 6) / N) exp(-2 pi i (m & 63) / N), about N / 64 + 64 values in shared memory).
+template <typename C> struct TwFull {
+    const C* t;
+    __device__ __forceinline__ C operator()(int m) const { return t[m]; }
+};
+template <typename C> struct TwTwoLevel {
+    const C* hi;
+    const C* lo;
+    __device__ __forceinline__ C operator()(int m) const { return cmul(hi[m >> 6], lo[m & 63]); }
+};
+
+template <typename T, int N, int NS, int R, class GE, bool SWZ_IN, class TW>
+__device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>* __restrict__ dst, const TW& tw,
+                                          int t) {
     static_assert(N % 8 == 0, "the stage swizzle permutes blocks of 8");
     using C = C_t<T>;
     constexpr int L = N / R;
@@ -345,7 +357,7 @@ __device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>
             }
             if (NS > 1) {
 #pragma unroll
-                for (int r = 1; r < R; r++) v[r] = cmul(v[r], tw[r * k * TSTEP]);
+                for (int r = 1; r < R; r++) v[r] = cmul(v[r], tw(r * k * TSTEP));
             }
             Dft<R, C>::run(v);
             const int ob = (j / NS) * NS * R + k;
@@ -356,18 +368,18 @@ __device__ __forceinline__ void stage_oop(const C_t<T>* __restrict__ src, C_t<T>
     __syncthreads();
 }
 
-template <typename T, int N, int NS, class GE, int R, int... Rest>
-__device__ __forceinline__ C_t<T>* fft_oop_(C_t<T>* a, C_t<T>* b, const C_t<T>* __restrict__ tw, int t) {
+template <typename T, int N, int NS, class GE, class TW, int R, int... Rest>
+__device__ __forceinline__ C_t<T>* fft_oop_(C_t<T>* a, C_t<T>* b, const TW& tw, int t) {
     stage_oop<T, N, NS, R, GE, (NS > 1)>(a, b, tw, t);
-    if constexpr (sizeof...(Rest) > 0) return fft_oop_<T, N, NS * R, GE, Rest...>(b, a, tw, t);
+    if constexpr (sizeof...(Rest) > 0) return fft_oop_<T, N, NS * R, GE, TW, Rest...>(b, a, tw, t);
     else return b;
 }
 
 // Result element k of pencil p sits at oop_swz(k) (see stage_oop).
-template <typename T, int N, class GE, int... Rs>
-__device__ __forceinline__ C_t<T>* fft_oop(C_t<T>* a, C_t<T>* b, const C_t<T>* __restrict__ tw, int t, Radix<Rs...>) {
+template <typename T, int N, class GE, class TW, int... Rs>
+__device__ __forceinline__ C_t<T>* fft_oop(C_t<T>* a, C_t<T>* b, const TW& tw, int t, Radix<Rs...>) {
     static_assert(sizeof...(Rs) > 0, "at least one stage");
-    return fft_oop_<T, N, 1, GE, Rs...>(a, b, tw, t);
+    return fft_oop_<T, N, 1, GE, TW, Rs...>(a, b, tw, t);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -180,6 +180,8 @@ template <typename T> struct ZArgs {
     double tq[3];                 // qC / (2 pi)
     AxisPlan zp;
     int* status;                  // device status word: bounded waits record timeouts here
+    long long ny;                 // yfast: the y extent
+    int yfast;                    // 1: fields laid out (x, k_z, y), y fastest (zstage_pfa only)
 };
 
 template <typename T, int NT, int EPT>
@@ -304,6 +306,7 @@ template <typename T> struct AxisArgs {
     long long nx, ny;
     int* status;        // device status word: bounded waits record timeouts here
     const double* gI;   // adjoint seed (EPI 2): dL/dI, fftshifted like I
+    int nouter;         // y-fastest x pass: the k_z extent (CTAs take k_z fastest)
 };
 
 // EPI 0: store the folded fields; 1: intensity epilogue; 2: adjoint seed, the conjugate gradient

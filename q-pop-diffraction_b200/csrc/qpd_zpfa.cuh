@@ -295,14 +295,32 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
                     }
                 }
                 __syncthreads();
-                C* o = a.out + 3LL * g * a.fstride + g0;
-                for (int e = tid; e < ncell; e += NT) {
-                    const int m = e / NZ;
-                    const int kz = e - m * NZ;
-                    const int s = m * PS + (kz % N1) * N2 + kz % N2;
-                    o[e] = cadd(buf[s], buf[3 * PLANE + s]);
-                    o[a.fstride + e] = buf[PLANE + s];
-                    o[2 * a.fstride + e] = buf[2 * PLANE + s];
+                if (a.yfast) {
+                    // (x, k_z, y) layout: column c = x ny + y goes to x nz ny + k_z ny + y; neighbouring
+                    // threads take neighbouring columns of one k_z (runs of up to M values)
+                    C* o = a.out + 3LL * g * a.fstride;
+                    const int mcols = ncell / NZ;
+                    for (int e = tid; e < ncell; e += NT) {
+                        const int kz = e / mcols;
+                        const int m = e - kz * mcols;
+                        const long long col = t * M + m;
+                        const long long x = col / a.ny, y = col - x * a.ny;
+                        const long long d = (x * NZ + kz) * a.ny + y;
+                        const int s = m * PS + (kz % N1) * N2 + kz % N2;
+                        o[d] = cadd(buf[s], buf[3 * PLANE + s]);
+                        o[a.fstride + d] = buf[PLANE + s];
+                        o[2 * a.fstride + d] = buf[2 * PLANE + s];
+                    }
+                } else {
+                    C* o = a.out + 3LL * g * a.fstride + g0;
+                    for (int e = tid; e < ncell; e += NT) {
+                        const int m = e / NZ;
+                        const int kz = e - m * NZ;
+                        const int s = m * PS + (kz % N1) * N2 + kz % N2;
+                        o[e] = cadd(buf[s], buf[3 * PLANE + s]);
+                        o[a.fstride + e] = buf[PLANE + s];
+                        o[2 * a.fstride + e] = buf[2 * PLANE + s];
+                    }
                 }
                 __syncthreads();
             }

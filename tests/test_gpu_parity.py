@@ -222,3 +222,32 @@ def test_prime_factor_z_stage_equals_stockham(gpu, monkeypatch, shape, weights):
     assert np.abs(out[0] - out[1]).max() / out[0].max() <= 1e-6
     ref = oracle.diffraction(*case.args())[0]
     assert_parity(out[1], ref, "fp32")
+
+
+def test_y_fastest_route_at_4000x4000x68(gpu, monkeypatch):
+    """The 4000 x 4000 x 68 route (z stage writing y-fastest fields, bulk y pass, swapped x pass)
+    against the z-fastest route of the same kernels, on the full config-3 volume."""
+    torch = gpu
+    free, _ = torch.cuda.mem_get_info(0)
+    if free < 160e9:
+        pytest.skip("needs about 150 GB of free device memory")
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    shape = (4000, 4000, 68)
+    params, inputs = workloads.gpu_snapshot("twin", shape, seed=3, device="cuda:0", n_phase=1)
+    crystal = crystal_from(params, workloads.config3_crystal(3, (1, 1, 3)))
+    out = torch.empty(shape, dtype=torch.float64, device="cuda:0")
+    for knob in ("0", "1"):
+        monkeypatch.setenv("QPOP_B200_YFAST", knob)
+        with Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp32") as plan:
+            plan.set_crystal(crystal)
+            plan.run_device(inputs, out)
+            torch.cuda.synchronize()
+            plan.device_status()
+        if knob == "0":
+            ref = out.clone()
+        else:
+            dmax = ((out - ref).abs().max() / ref.max()).item()
+            assert dmax <= 1e-6, dmax
+            # the routes round differently (two-level twiddles in the bulk y pass): identical bits would
+            # mean the y-fastest route did not run
+            assert not torch.equal(out, ref)
