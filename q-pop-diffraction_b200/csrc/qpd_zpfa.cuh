@@ -300,11 +300,15 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
                     // threads take neighbouring columns of one k_z (runs of up to M values)
                     C* o = a.out + 3LL * g * a.fstride;
                     const int mcols = ncell / NZ;
+                    const long long x0 = t * M / a.ny, y0 = t * M - x0 * a.ny;  // the tile's first column
                     for (int e = tid; e < ncell; e += NT) {
-                        const int kz = e / mcols;
+                        const int kz = mcols == M ? e / M : e / mcols;  // full tiles divide by a constant
                         const int m = e - kz * mcols;
-                        const long long col = t * M + m;
-                        const long long x = col / a.ny, y = col - x * a.ny;
+                        long long x = x0, y = y0 + m;
+                        if (y >= a.ny) {  // M < ny: a tile wraps into the next x row at most once
+                            y -= a.ny;
+                            x += 1;
+                        }
                         const long long d = (x * NZ + kz) * a.ny + y;
                         const int s = m * PS + (kz % N1) * N2 + kz % N2;
                         o[d] = cadd(buf[s], buf[3 * PLANE + s]);
