@@ -12,6 +12,12 @@
 
 namespace qpd {
 
+// Position of index k (< n) after fftshift: (k + n / 2) mod n with one conditional subtraction.
+__device__ __forceinline__ int fftshift_at(int k, int n) {
+    const int v = k + n / 2;
+    return v >= n ? v - n : v;
+}
+
 // ---------------------------------------------------------------------------------------
 // z stage: source + FFT along z + fold, M columns of NZ cells per CTA
 // ---------------------------------------------------------------------------------------
@@ -196,7 +202,7 @@ __global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
                     const int kx = e / CV;
                     const int c = (e - kx * CV) * VEC;
                     const double sxy = a.S[0][kx] * syv;
-                    const long long row = ((kx + a.nx / 2) % a.nx * a.ny + sy) * a.nz;
+                    const long long row = ((long long)fftshift_at(kx, (int)a.nx) * a.ny + sy) * a.nz;
 #pragma unroll
                     for (int w = 0; w < VEC; w++) {
                         const int kz = z0 + c + w;
@@ -204,7 +210,7 @@ __global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
                             const double S = sxy * a.S[2][kz];
                             const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
                             const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
-                            a.I[row + (kz + a.nz / 2) % a.nz] = v;
+                            a.I[row + fftshift_at(kz, a.nz)] = v;
                         }
                     }
                 }
@@ -400,7 +406,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                     const int kx = e / CV;
                     const int c = (e - kx * CV) * VEC;
                     const double sxz = a.S[0][kx] * szv;
-                    const long long row = (kx + a.nx / 2) % a.nx * a.ny;
+                    const long long row = (long long)fftshift_at(kx, (int)a.nx) * a.ny;
 #pragma unroll
                     for (int w = 0; w < VEC; w++) {
                         const int ky = z0 + c + w;
@@ -408,7 +414,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                             const double S = sxz * a.S[1][ky];
                             const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
                             const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
-                            a.I[(row + (ky + a.ny / 2) % a.ny) * nzr + sz] = v;
+                            a.I[(row + fftshift_at(ky, (int)a.ny)) * nzr + sz] = v;
                         }
                     }
                 }
@@ -424,7 +430,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                     const int kx = e / CV;
                     const int c = (e - kx * CV) * VEC;
                     const double sxy = a.S[0][kx] * syv;
-                    const long long row = ((kx + a.nx / 2) % a.nx * a.ny + sy) * a.nz;
+                    const long long row = ((long long)fftshift_at(kx, (int)a.nx) * a.ny + sy) * a.nz;
 #pragma unroll
                     for (int w = 0; w < VEC; w++) {
                         const int kz = z0 + c + w;
@@ -432,7 +438,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                             const double S = sxy * a.S[2][kz];
                             const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
                             const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
-                            a.I[row + (kz + a.nz / 2) % a.nz] = v;
+                            a.I[row + fftshift_at(kz, a.nz)] = v;
                         }
                     }
                 }
