@@ -194,8 +194,9 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"two-phase vortex film {'x'.join(map(str, GRID))}, 5 atoms, G=002,103",
-                   "sample": sample},
+        "config": {"workload": f"two-phase polar-vortex film {'x'.join(map(str, GRID))}, 5 atoms, 2 phases, "
+                               f"G=002,103 alternating", "grid": list(GRID), "cells": int(np.prod(GRID)), "atoms": 5,
+                   "phases": 2, "precision": "fp64 (NumPy, as the reference computes)", "sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
