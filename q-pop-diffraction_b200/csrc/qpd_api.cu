@@ -105,7 +105,9 @@ struct qpd_ctx {
     // QPOP_B200_YFAST=0: keep the z-fastest field layout at 4000 x 4000 x 68 (the y-fastest route writes
     // the z stage's fields with y fastest so the 4000-point y transforms read contiguous pencils)
     int knob_yfast = 1;
-    int knob_bulk_nt = 256;  // QPOP_B200_BULK_NT: threads of the bulk y pass (256: 72.8 ms, 512: 80.9 ms)
+    int knob_bulk_nt = 256;
+    // QPOP_B200_ADJ_TMA=0: the adjoint's x and y passes on the generic kernels instead of the TMA one
+    int knob_adj_tma = 1;  // QPOP_B200_BULK_NT: threads of the bulk y pass (256: 72.8 ms, 512: 80.9 ms)
     // QPOP_B200_OOP=0: in-place stages for the 256- and 512-point TMA passes (out-of-place measured
     // 1.080 against 1.104 ms for the y pass at 512x512x104)
     int knob_oop = 1;
@@ -667,7 +669,24 @@ template <typename T> struct Impl {
         return tstop(c, QPD_K_ADJAXIS, st, t0);
     }
 
-    static int run_adj_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, cudaStream_t st) {
+    // adjoint x / y pass on the TMA kernel (coefficients before the transform), for the lengths the
+    // forward specialises; nfields_in: fields of the adjoint workspace the input lives in
+    template <int N, int NT, class RAD>
+    static int adj_tma_(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, bool xp, cudaStream_t st, int64_t nfields_in) {
+        if (xp) return tma_axis_b<N, 8, NT, 2, false, true, RAD, 2, true, false, true>(c, a, nouter, QPD_K_ADJAXIS, st,
+                                                                                   nfields_in);
+        return tma_axis_b<N, 8, NT, 2, false, false, RAD, 2, true, false, true>(c, a, nouter, QPD_K_ADJAXIS, st,
+                                                                             nfields_in);
+    }
+
+    static int run_adj_axis(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, cudaStream_t st, bool xp = false,
+                            int64_t nfields_in = 0) {
+        if constexpr (sizeof(T) == 4) {
+            if (c->fast && c->tma && c->knob_adj_tma && nfields_in > 0 && a.nz % 2 == 0) {
+                if (a.N == 256) return adj_tma_<256, 256, Radix<8, 8, 4>>(c, a, nouter, xp, st, nfields_in);
+                if (a.N == 512) return adj_tma_<512, 512, Radix<8, 8, 8>>(c, a, nouter, xp, st, nfields_in);
+            }
+        }
         const size_t lim = max_smem(c);
         int best = -1, bestCz = 0;
         for (int i = 0; i < 4; i++) {
@@ -835,23 +854,26 @@ template <typename T> struct Impl {
     }
 
     // YZ: the x pass over fields laid out (x, k_z, y): a.nz is then the y extent and nouter the k_z extent
-    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF, bool OOP = false, bool YZ = false>
-    static int tma_axis_b(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st) {
+    // nfields_in: fields of the input buffer the tensor map covers (default: the forward's field workspace)
+    template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF, bool OOP = false, bool YZ = false,
+              bool PRE = false>
+    static int tma_axis_b(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st,
+                          int64_t nfields_in = -1) {
         constexpr int BOX = tma_rows(N, CZ * (int)sizeof(C));
         a.Cz = CZ;
         a.nzc = (a.nz + CZ - 1) / CZ;
         a.nouter = (int)nouter;
         CUtensorMap map;
-        const int64_t nfields = c->sched_used == QPD_SCHED_FUSED ? 3 * c->ng1 : 2;
+        const int64_t nfields = nfields_in > 0 ? nfields_in : c->sched_used == QPD_SCHED_FUSED ? 3 * c->ng1 : 2;
         QPD_TRY(field_map(c, &map, const_cast<C*>(a.in), sizeof(T) == 8, a.nz, YZ ? c->nz : c->ny, nfields * c->nx,
                           2 * CZ, XP ? 1 : BOX, XP ? BOX : 1));
         const size_t smem = sizeof(C) * N * CZ * (NBUF + (OOP ? 1 : 0)) + sizeof(C) * N + 128;
         if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "axis tile exceeds shared memory");
-        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ>, smem));
+        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ, PRE>, smem));
         const int64_t grid = nouter * a.nzc;
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
-        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ><<<(unsigned)grid, NT, smem, st>>>(map, a);
+        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ, PRE><<<(unsigned)grid, NT, smem, st>>>(map, a);
         return tstop(c, kind, st, t0);
     }
 
@@ -1025,7 +1047,10 @@ template <typename T> struct Impl {
         ax.segs = tab<Segment<T>>(c, c->off_segAX);
         ax.nseg = c->nsegAX;
         ax.ap = axis_plan(c, 0);
-        QPD_TRY(run_adj_axis(c, ax, c->ny, st));
+        ax.nx = c->nx;
+        ax.ny = c->ny;
+        ax.status = static_cast<int*>(c->status.p);
+        QPD_TRY(run_adj_axis(c, ax, c->ny, st, true, 1 + 2 * c->ng2));
 
         AxisArgs<T> ay;
         std::memset(&ay, 0, sizeof ay);
@@ -1039,7 +1064,10 @@ template <typename T> struct Impl {
         ay.segs = tab<Segment<T>>(c, c->off_segAY);
         ay.nseg = c->nsegAY;
         ay.ap = axis_plan(c, 1);
-        QPD_TRY(run_adj_axis(c, ay, c->nx, st));
+        ay.nx = c->nx;
+        ay.ny = c->ny;
+        ay.status = static_cast<int*>(c->status.p);
+        QPD_TRY(run_adj_axis(c, ay, c->nx, st, false, 1 + 2 * c->ng2));
 
         AdjZArgs<T> az;
         std::memset(&az, 0, sizeof az);
@@ -1540,6 +1568,7 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     if (const char* k = std::getenv("QPOP_B200_N4000")) c->knob_n4000 = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_OOP")) c->knob_oop = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_YFAST")) c->knob_yfast = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_ADJ_TMA")) c->knob_adj_tma = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_BULK_NT")) c->knob_bulk_nt = std::atoi(k) == 512 ? 512 : 256;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {

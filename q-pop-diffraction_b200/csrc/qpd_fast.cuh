@@ -269,8 +269,10 @@ __host__ __device__ constexpr int tma_rows(int N, int row_bytes) {
 // one butterfly in registers at a time); the in-place stages otherwise.
 // YZ (x pass with EPI only): the fields are laid out (x, k_z, y) with y fastest, so a tile holds CZ
 // values of k_y at one k_z; CTAs take k_z fastest, so the CTAs writing neighbouring z of I run together.
+// PRE (the adjoint's passes, one input per segment): the coefficients multiply the tile before the
+// transform and the transformed tile is the output.
 template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF, bool OOP = false,
-          bool YZ = false>
+          bool YZ = false, bool PRE = false>
 __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (NBUF + (OOP ? 1 : 0)) + N) <= 110 * 1024 ? 2 : 1)
     axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
     using C = C_t<T>;
@@ -291,6 +293,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
     C* scratch = tw + N;         // OOP: the second buffer of the out-of-place stages
     __shared__ __align__(8) uint64_t bar[NBUF];
     static_assert(!YZ || (EPI && XPASS), "the y-fastest layout is read by the x pass only");
+    static_assert(!PRE || (!EPI && !YZ), "the pre-multiplied passes store fields");
     const int tid = threadIdx.x;
     const long long outer = YZ ? blockIdx.x % a.nouter : blockIdx.x / a.nzc;
     const int z0 = (int)(YZ ? blockIdx.x / a.nouter : blockIdx.x % a.nzc) * CZ;
@@ -365,6 +368,12 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                         mbar_wait(&bar[(fl + k) % NBUF], ((fl + k) / NBUF) & 1, nullptr);
                 return;
             }
+            if constexpr (PRE) {
+                if (cf) {
+                    for (int e = tid; e < TILE; e += NT) buf[e] = cmul(cf[e / CZ], buf[e]);
+                    __syncthreads();
+                }
+            }
             C* res = buf;
             if constexpr (OOP) res = fft_oop<T, N, GE>(buf, scratch, TwFull<C>{tw}, tid, RAD{});
             else fft_ct<T, N, GE>(buf, tw, tid, RAD{});
@@ -377,7 +386,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                         const int k = e / CV;
                         const int c = (e - k * CV) * VEC;
                         const C* s = res + (OOP ? oop_swz(k) : k) * CZ + c;
-                        if (seg.ident) {
+                        if (PRE || seg.ident) {
 #pragma unroll
                             for (int w = 0; w < VEC; w++) acc[0][q][w] = cadd(acc[0][q][w], s[w]);
                         } else {
