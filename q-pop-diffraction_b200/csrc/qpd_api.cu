@@ -856,7 +856,7 @@ template <typename T> struct Impl {
     // YZ: the x pass over fields laid out (x, k_z, y): a.nz is then the y extent and nouter the k_z extent
     // nfields_in: fields of the input buffer the tensor map covers (default: the forward's field workspace)
     template <int N, int CZ, int NT, int VEC, bool EPI, bool XP, class RAD, int NBUF, bool OOP = false, bool YZ = false,
-              bool PRE = false>
+              bool PRE = false, bool SEED = false>
     static int tma_axis_b(qpd_ctx* c, AxisArgs<T>& a, int64_t nouter, int kind, cudaStream_t st,
                           int64_t nfields_in = -1) {
         constexpr int BOX = tma_rows(N, CZ * (int)sizeof(C));
@@ -869,11 +869,11 @@ template <typename T> struct Impl {
                           2 * CZ, XP ? 1 : BOX, XP ? BOX : 1));
         const size_t smem = sizeof(C) * N * CZ * (NBUF + (OOP ? 1 : 0)) + sizeof(C) * N + 128;
         if (smem > max_smem(c)) return fail(c, QPD_ERR_UNSUPPORTED, "axis tile exceeds shared memory");
-        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ, PRE>, smem));
+        QPD_TRY(set_smem(c, axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ, PRE, SEED>, smem));
         const int64_t grid = nouter * a.nzc;
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
-        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ, PRE><<<(unsigned)grid, NT, smem, st>>>(map, a);
+        axis_tma<T, N, CZ, NT, VEC, EPI, XP, RAD, NBUF, OOP, YZ, PRE, SEED><<<(unsigned)grid, NT, smem, st>>>(map, a);
         return tstop(c, kind, st, t0);
     }
 
@@ -1033,7 +1033,22 @@ template <typename T> struct Impl {
         AxisArgs<T> x = xargs(c);
         x.out = W;
         x.gI = dI;
-        QPD_TRY(run_axis<2>(c, x, c->ny, QPD_K_ADJSEED, st));
+        bool seeded = false;
+        if constexpr (sizeof(T) == 4) {
+            if (c->fast && c->tma && c->knob_adj_tma && c->nz % 2 == 0) {
+                using namespace qpd;
+                if (c->nx == 256) {
+                    QPD_TRY((tma_axis_b<256, 8, 256, 2, true, true, Radix<8, 8, 4>, 2, true, false, false, true>(
+                        c, x, c->ny, QPD_K_ADJSEED, st)));
+                    seeded = true;
+                } else if (c->nx == 512) {
+                    QPD_TRY((tma_axis_b<512, 8, 512, 2, true, true, Radix<8, 8, 8>, 2, true, false, false, true>(
+                        c, x, c->ny, QPD_K_ADJSEED, st)));
+                    seeded = true;
+                }
+            }
+        }
+        if (!seeded) QPD_TRY(run_axis<2>(c, x, c->ny, QPD_K_ADJSEED, st));
 
         AxisArgs<T> ax;
         std::memset(&ax, 0, sizeof ax);

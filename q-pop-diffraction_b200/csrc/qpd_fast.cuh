@@ -271,8 +271,10 @@ __host__ __device__ constexpr int tma_rows(int N, int row_bytes) {
 // values of k_y at one k_z; CTAs take k_z fastest, so the CTAs writing neighbouring z of I run together.
 // PRE (the adjoint's passes, one input per segment): the coefficients multiply the tile before the
 // transform and the transformed tile is the output.
+// SEED (with EPI): the adjoint's seed instead of the intensity, D = dL/dI S^2 conj(Amp) / (n V) (0 where
+// I is at its floor) written as field seg.out[0] of a.out, in the unshifted field layout.
 template <typename T, int N, int CZ, int NT, int VEC, bool EPI, bool XPASS, class RAD, int NBUF, bool OOP = false,
-          bool YZ = false, bool PRE = false>
+          bool YZ = false, bool PRE = false, bool SEED = false>
 __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (NBUF + (OOP ? 1 : 0)) + N) <= 110 * 1024 ? 2 : 1)
     axis_tma(const __grid_constant__ CUtensorMap map, AxisArgs<T> a) {
     using C = C_t<T>;
@@ -294,6 +296,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
     __shared__ __align__(8) uint64_t bar[NBUF];
     static_assert(!YZ || (EPI && XPASS), "the y-fastest layout is read by the x pass only");
     static_assert(!PRE || (!EPI && !YZ), "the pre-multiplied passes store fields");
+    static_assert(!SEED || (EPI && XPASS && !YZ), "the seed is an x-pass epilogue");
     const int tid = threadIdx.x;
     const long long outer = YZ ? blockIdx.x % a.nouter : blockIdx.x / a.nzc;
     const int z0 = (int)(YZ ? blockIdx.x / a.nouter : blockIdx.x % a.nzc) * CZ;
@@ -402,7 +405,34 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                 issue(fl + NBUF, b);
             }
         }
-        if constexpr (EPI && YZ) {
+        if constexpr (EPI && SEED) {
+            const long long ky = outer;
+            const int sy = fftshift_at((int)ky, (int)a.ny);
+            const double syv = a.S[1][ky];
+            C* dst = a.out + seg.out[0] * a.fstride + base;
+#pragma unroll
+            for (int q = 0; q < EP; q++) {
+                const int e = tid + q * NT;
+                if (GROUPS % NT == 0 || e < GROUPS) {
+                    const int kx = e / CV;
+                    const int c = (e - kx * CV) * VEC;
+                    const double sxy = a.S[0][kx] * syv;
+                    const long long row = ((long long)fftshift_at(kx, (int)a.nx) * a.ny + sy) * a.nz;
+#pragma unroll
+                    for (int w = 0; w < VEC; w++) {
+                        const int kz = z0 + c + w;
+                        if (c + w < cz) {
+                            const double S = sxy * a.S[2][kz];
+                            const double S2 = S * S * a.scale2;
+                            const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
+                            double f = 0.0;
+                            if (S2 * (re * re + im * im) > 1e-50) f = a.gI[row + fftshift_at(kz, a.nz)] * S2;
+                            dst[kx * a.stride + c + w] = cmake<C>(T(f * re), T(-f * im));
+                        }
+                    }
+                }
+            }
+        } else if constexpr (EPI && YZ) {
             // outer = k_z, z0 + c + w = k_y; I is (x, y, z) with z fastest
             const long long nzr = a.nouter;
             const long long kz = outer;
