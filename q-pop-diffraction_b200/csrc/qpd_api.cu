@@ -722,6 +722,20 @@ template <typename T> struct Impl {
         return tstop(c, QPD_K_ADJZ, st, t0);
     }
 
+    template <int NZ, int M, int NT, class RAD> static int adj_z_fast_(qpd_ctx* c, AdjZArgs<T>& a, cudaStream_t st) {
+        constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+        a.z.M = M;
+        a.z.ps = PS;
+        const size_t smem = sizeof(C) * 4 * M * PS + sizeof(AtomPhase<T>) * a.z.in.nPhase * a.z.nAtom + 16;
+        if (smem > max_smem(c)) return run_adj_z(c, a, st);
+        QPD_TRY(set_smem(c, adj_zstage_fast<T, NZ, M, NT, RAD>, smem));
+        const int64_t grid = (a.z.ncols + M - 1) / M;
+        cudaEvent_t t0;
+        QPD_TRY(tstart(c, st, &t0));
+        adj_zstage_fast<T, NZ, M, NT, RAD><<<(unsigned)grid, NT, smem, st>>>(a);
+        return tstop(c, QPD_K_ADJZ, st, t0);
+    }
+
     static int run_adj_z(qpd_ctx* c, AdjZArgs<T>& a, cudaStream_t st) {
         const size_t lim = max_smem(c);
         for (const Cfg& f : kZCfg) {
@@ -1091,6 +1105,12 @@ template <typename T> struct Impl {
         az.dU = dU;
         az.dP = dP;
         for (int d = 0; d < 3; d++) az.qc[d] = 2.0 * M_PI * c->tq[d];
+        if constexpr (sizeof(T) == 4) {
+            if (c->fast && c->knob_adj_tma && !in.wdense) {
+                if (c->nz == 64) return adj_z_fast_<64, 16, 256, Radix<8, 8>>(c, az, st);
+                if (c->nz == 104) return adj_z_fast_<104, 8, 256, Pfa<8, 13>>(c, az, st);
+            }
+        }
         return run_adj_z(c, az, st);
     }
 

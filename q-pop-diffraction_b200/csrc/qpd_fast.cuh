@@ -516,6 +516,98 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
 }
 
 // ---------------------------------------------------------------------------------------
+// Adjoint z stage with a compile-time transform (the adj_zstage_kernel of qpd_kernels.cuh for the
+// lengths the forward specialises): per atom, the group's 3 conjugate adjoint fields times the z
+// factors become 4 pencils per column, transformed along z in shared memory; each cell then adds
+// its source transpose to dL/du and dL/dP held in registers.
+// ---------------------------------------------------------------------------------------
+template <typename T, int NZ, int M, int NT, class RAD>
+__global__ void __launch_bounds__(NT) adj_zstage_fast(AdjZArgs<T> a) {
+    using C = C_t<T>;
+    constexpr int PS = NZ % 2 ? NZ : NZ + 1;
+    constexpr int PLANE = M * PS;
+    constexpr int CELLS = M * NZ;
+    constexpr int CPT = cdiv(CELLS, NT);
+    using GE = Geo<4 * M, 4 * M, PS, 0, 1, NT>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    C* buf = reinterpret_cast<C*>(smem_raw);
+    const ZArgs<T>& z = a.z;
+    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(buf + 4 * PLANE);
+    const int tid = threadIdx.x;
+    const int nap = z.in.nPhase * z.nAtom;
+    for (int i = tid; i < nap; i += NT) apc[i] = z.apc[i];
+    const long long c0 = (long long)blockIdx.x * M;
+    const int ncell = (int)min((long long)M, z.ncols - c0) * NZ;
+    const long long g0 = c0 * NZ;
+    const C* tw = static_cast<const C*>(z.zp.tw);
+
+    CellIn<T> cell[CPT];
+    int ph[CPT];
+    T wt[CPT], dU[CPT][3], dP[CPT][3];
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int e = tid + q * NT;
+        ph[q] = -1;
+        wt[q] = T(0);
+#pragma unroll
+        for (int d = 0; d < 3; d++) dU[q][d] = dP[q][d] = T(0);
+        if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+            const long long g = g0 + e;
+            load_cell<T>(z.in, g, z.tq, cell[q]);
+            ph[q] = z.in.phase[g];
+            wt[q] = z.in.weight ? z.in.weight[g] : T(1);
+        }
+    }
+    __syncthreads();
+    for (int at = 0; at < z.nAtom; at++) {
+        const C* fa = a.fin + 3LL * z.grp[at] * z.fstride + g0;
+        const C* ce = z.coefE + (long long)at * NZ;
+        const C* cu = z.coefUz + (long long)at * NZ;
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                const int m = e / NZ;
+                const int kz = e - m * NZ;
+                const int s = m * PS + kz;
+                const C A = fa[e], X = fa[z.fstride + e], Y = fa[2 * z.fstride + e];
+                const C e1 = ce[kz], u1 = cu[kz];
+                buf[s] = cmul(e1, A);
+                buf[PLANE + s] = cmul(e1, X);
+                buf[2 * PLANE + s] = cmul(e1, Y);
+                buf[3 * PLANE + s] = cmul(u1, A);
+            }
+        }
+        __syncthreads();
+        fft_ct<T, NZ, GE>(buf, tw, tid, RAD{});
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                const int m = e / NZ;
+                const int s = m * PS + OutPos<RAD>::at(e - m * NZ);
+                if (ph[q] >= 0 && ph[q] < z.in.nPhase)
+                    add_adjoint<T>(cell[q], apc[ph[q] * z.nAtom + at], wt[q], a.qc, buf[s], buf[PLANE + s],
+                                   buf[2 * PLANE + s], buf[3 * PLANE + s], dU[q], dP[q]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < CPT; q++) {
+        const int e = tid + q * NT;
+        if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+            const long long g = g0 + e;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                a.dU[d * z.in.n + g] = dU[q][d];
+                a.dP[d * z.in.n + g] = d < z.in.nStruc ? dP[q][d] : T(0);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // y pass over fields laid out (x, k_z, y), y fastest: one pencil (x, k_z) of N contiguous values per
 // CTA.  Each input field's pencil arrives by 1-D bulk copies in one of two buffers while the
 // previous field is transformed (out-of-place swizzled stages through a third buffer, twiddles from

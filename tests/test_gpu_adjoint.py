@@ -67,7 +67,8 @@ def rel(a, b):
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("fp32", 2e-3)])
 @pytest.mark.parametrize("shape,weights,nPhase", [((24, 20, 16), "dense", 2), ((16, 12, 10), "onehot", 2),
-                                                  ((20, 8, 13), "region", 1)])
+                                                  ((20, 8, 13), "region", 1), ((12, 10, 104), "onehot", 2),
+                                                  ((10, 12, 64), "region", 1)])
 def test_adjoint_matches_complex128_autograd(gpu, precision, tol, shape, weights, nPhase):
     torch = gpu
     plan, crystal, packed, target, W, _ = problem(torch, shape, precision, seed=sum(shape), weights=weights,
