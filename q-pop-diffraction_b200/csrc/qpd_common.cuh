@@ -34,6 +34,65 @@ template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s)
 template <typename C> __device__ __forceinline__ C cmul_mi(C a) { return cmake<C>(a.y, -a.x); }
 // +i * a
 template <typename C> __device__ __forceinline__ C cmul_pi(C a) { return cmake<C>(-a.y, a.x); }
+// a - i b and a + i b (the swap stays in the scalar operands)
+template <typename C> __device__ __forceinline__ C cadd_mi(C a, C b) { return cmake<C>(a.x + b.y, a.y - b.x); }
+template <typename C> __device__ __forceinline__ C cadd_pi(C a, C b) { return cmake<C>(a.x - b.y, a.y + b.x); }
+// a += s * b, s real
+template <typename C> __device__ __forceinline__ void caxpy(C& a, decltype(C::x) s, C b) {
+    a.x = fma(s, b.x, a.x);
+    a.y = fma(s, b.y, a.y);
+}
+
+#ifndef QPD_F32X2
+#define QPD_F32X2 1
+#endif
+#if QPD_F32X2 && defined(__CUDA_ARCH__)
+// complex64 on the packed two-lane float32 instructions of sm_100 (add/sub/mul/fma .f32x2): one
+// instruction per complex add or real-scaled multiply-add instead of two.  Same IEEE round-to-
+// nearest results per lane as the scalar forms.
+__device__ __forceinline__ unsigned long long f2_pk(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2_up(unsigned long long r) {
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_pk(a)), "l"(f2_pk(b)));
+    return f2_up(d);
+}
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_pk(a)), "l"(f2_pk(b)));
+    return f2_up(d);
+}
+template <> __device__ __forceinline__ float2 cscale<float2>(float2 a, float s) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_pk(a)), "l"(f2_pk(make_float2(s, s))));
+    return f2_up(d);
+}
+template <> __device__ __forceinline__ void caxpy<float2>(float2& a, float s, float2 b) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_pk(make_float2(s, s))), "l"(f2_pk(b)), "l"(f2_pk(a)));
+    a = f2_up(d);
+}
+// a += b * c: the b.x products as one packed fma, the b.y cross terms scalar
+template <> __device__ __forceinline__ void cfma<float2>(float2& a, float2 b, float2 c) {
+    caxpy(a, b.x, c);
+    a.x = fmaf(-b.y, c.y, a.x);
+    a.y = fmaf(b.y, c.x, a.y);
+}
+template <> __device__ __forceinline__ float2 cmul<float2>(float2 a, float2 b) {
+    float2 t = cscale(b, a.x);
+    t.x = fmaf(-a.y, b.y, t.x);
+    t.y = fmaf(a.y, b.x, t.y);
+    return t;
+}
+#endif
 
 
 }  // namespace qpd

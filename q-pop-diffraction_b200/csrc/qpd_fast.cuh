@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
 // its source transpose to dL/du and dL/dP held in registers.
 // ---------------------------------------------------------------------------------------
 template <typename T, int NZ, int M, int NT, class RAD>
-__global__ void __launch_bounds__(NT) adj_zstage_fast(AdjZArgs<T> a) {
+__global__ void __launch_bounds__(NT, 2) adj_zstage_fast(AdjZArgs<T> a) {
     using C = C_t<T>;
     constexpr int PS = NZ % 2 ? NZ : NZ + 1;
     constexpr int PLANE = M * PS;

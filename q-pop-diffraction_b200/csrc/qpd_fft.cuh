@@ -63,13 +63,11 @@ template <int R, typename C> struct Dft {
                 const C w = unit_root<T>(root_offset(R) + (r * s) % R);
                 const T c = w.x;
                 const T sn = -w.y;
-                A.x = fma(c, a[r - 1].x, A.x);
-                A.y = fma(c, a[r - 1].y, A.y);
-                B.x = fma(sn, b[r - 1].x, B.x);
-                B.y = fma(sn, b[r - 1].y, B.y);
+                caxpy(A, c, a[r - 1]);
+                caxpy(B, sn, b[r - 1]);
             }
-            x[s] = cadd(A, cmul_mi(B));
-            x[R - s] = cadd(A, cmul_pi(B));
+            x[s] = cadd_mi(A, B);
+            x[R - s] = cadd_pi(A, B);
         }
         x[0] = y0;
     }
@@ -91,17 +89,17 @@ template <typename C> struct Dft<3, C> {
         C m = cmake<C>(x[0].x - R_t(0.5) * t.x, x[0].y - R_t(0.5) * t.y);
         C d = cscale(csub(x[1], x[2]), h);
         x[0] = cadd(x[0], t);
-        x[1] = cadd(m, cmul_mi(d));
-        x[2] = cadd(m, cmul_pi(d));
+        x[1] = cadd_mi(m, d);
+        x[2] = cadd_pi(m, d);
     }
 };
 
 template <typename C> __device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
-    C a = cadd(x0, x2), b = csub(x0, x2), c = cadd(x1, x3), d = cmul_mi(csub(x1, x3));
+    C a = cadd(x0, x2), b = csub(x0, x2), c = cadd(x1, x3), d = csub(x1, x3);
     x0 = cadd(a, c);
     x2 = csub(a, c);
-    x1 = cadd(b, d);
-    x3 = csub(b, d);
+    x1 = cadd_mi(b, d);  // b - i d
+    x3 = cadd_pi(b, d);
 }
 
 template <typename C> struct Dft<4, C> {
@@ -117,14 +115,13 @@ template <typename C> struct Dft<8, C> {
         dft4(e0, e1, e2, e3);
         dft4(o0, o1, o2, o3);
         C t1 = cmake<C>((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);   // exp(-i pi / 4) o1
-        C t2 = cmul_mi(o2);                                         // exp(-i pi / 2) o2
         C t3 = cmake<C>((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);  // exp(-3 i pi / 4) o3
         x[0] = cadd(e0, o0);
         x[4] = csub(e0, o0);
         x[1] = cadd(e1, t1);
         x[5] = csub(e1, t1);
-        x[2] = cadd(e2, t2);
-        x[6] = csub(e2, t2);
+        x[2] = cadd_mi(e2, o2);  // exp(-i pi / 2) o2
+        x[6] = cadd_pi(e2, o2);
         x[3] = cadd(e3, t3);
         x[7] = csub(e3, t3);
     }
