@@ -251,3 +251,45 @@ def test_y_fastest_route_at_4000x4000x68(gpu, monkeypatch):
             # the routes round differently (two-level twiddles in the bulk y pass): identical bits would
             # mean the y-fastest route did not run
             assert not torch.equal(out, ref)
+
+
+def test_direct_sum_voxels_at_4000x4000x68(gpu):
+    """The full 4000 x 4000 x 68 volume (default route) against float64 direct sums over all 1.088e9
+    cells at 64 voxels: the 32 brightest of the result and 32 drawn at random.  Independent of every
+    FFT kernel; the per-precision contract is the float32 one of the smaller grids."""
+    torch = gpu
+    free, _ = torch.cuda.mem_get_info(0)
+    if free < 160e9:
+        pytest.skip("needs about 150 GB of free device memory")
+    from direct_dft import crystal_constants, direct_intensity, fft_index_to_shifted, shifted_to_fft_index
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    shape = (4000, 4000, 68)
+    params, inputs = workloads.gpu_snapshot("twin", shape, seed=3, device="cuda:0", n_phase=1)
+    atoms = workloads.config3_crystal(3, (1, 1, 3))
+    out = torch.empty(shape, dtype=torch.float64, device="cuda:0")
+    with Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp32") as plan:
+        plan.set_crystal(crystal_from(params, atoms))
+        plan.run_device(inputs, out)
+        torch.cuda.synchronize()
+        plan.device_status()
+    top = torch.topk(out.view(-1), 32).indices.cpu().numpy()
+    sx, sy, sz = np.unravel_index(top, shape)
+    inv = [shifted_to_fft_index(s) for s in shape]
+    bright = np.stack([inv[0][sx], inv[1][sy], inv[2][sz]], axis=1)
+    rng = np.random.default_rng(11)
+    rand = np.stack([rng.integers(0, s, 32) for s in shape], axis=1)
+    vox = np.concatenate([bright, rand])
+    pos = [fft_index_to_shifted(s) for s in shape]
+    sel = [torch.from_numpy(pos[d][vox[:, d]]).to(out.device) for d in range(3)]
+    got = out[sel[0], sel[1], sel[2]].cpu().numpy()
+    del out
+    torch.cuda.empty_cache()
+    spacing = (params.dx, params.dy, params.dz)
+    want = direct_intensity(torch, shape, spacing, *crystal_constants(params, atoms), inputs["P"], inputs["U"],
+                            inputs["phase"], inputs["weight"], vox)
+    Imax = want.max()
+    big = want > 1e-6 * Imax
+    dmax = np.abs(got - want).max() / Imax
+    rel = (np.abs(got - want)[big] / want[big]).max()
+    print(f"direct sums at {len(vox)} voxels: max |dI|/I_max {dmax:.2e}, max rel {rel:.2e} over {big.sum()} voxels")
+    assert dmax <= 1e-5 and big.sum() >= 32 and rel <= 1e-3, (dmax, rel, big.sum())
