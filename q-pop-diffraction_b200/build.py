@@ -51,14 +51,18 @@ def build(force=False, verbose=False, extra=()):
     """Compile every CUDA source into libqpopdiff.so next to this file; returns its path."""
     if not force and up_to_date():
         return LIB
-    tmp = LIB.with_suffix(".so.tmp")
+    # per-process temporary: concurrent builds each write their own file and the last rename wins
+    tmp = LIB.with_suffix(f".so.tmp{os.getpid()}")
     cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", str(INCLUDE), "-I", str(CSRC),
            "-DQPD_BUILD", *extra, *map(str, sources()), "-o", str(tmp)]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
+    try:
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, LIB)
+    finally:
+        tmp.unlink(missing_ok=True)
     return LIB
 
 
