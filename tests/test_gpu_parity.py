@@ -228,6 +228,7 @@ def test_y_fastest_route_at_4000x4000x68(gpu, monkeypatch):
     """The 4000 x 4000 x 68 route (z stage writing y-fastest fields, bulk y pass, swapped x pass)
     against the z-fastest route of the same kernels, on the full config-3 volume."""
     torch = gpu
+    torch.cuda.empty_cache()  # blocks an earlier test left in the caching allocator
     free, _ = torch.cuda.mem_get_info(0)
     if free < 160e9:
         pytest.skip("needs about 150 GB of free device memory")
@@ -258,6 +259,7 @@ def test_direct_sum_voxels_at_4000x4000x68(gpu):
     cells at 64 voxels: the 32 brightest of the result and 32 drawn at random.  Independent of every
     FFT kernel; the per-precision contract is the float32 one of the smaller grids."""
     torch = gpu
+    torch.cuda.empty_cache()  # blocks an earlier test left in the caching allocator
     free, _ = torch.cuda.mem_get_info(0)
     if free < 160e9:
         pytest.skip("needs about 150 GB of free device memory")
