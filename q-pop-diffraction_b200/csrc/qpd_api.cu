@@ -726,7 +726,8 @@ template <typename T> struct Impl {
         constexpr int PS = NZ % 2 ? NZ : NZ + 1;
         a.z.M = M;
         a.z.ps = PS;
-        const size_t smem = sizeof(C) * 4 * M * PS + sizeof(AtomPhase<T>) * a.z.in.nPhase * a.z.nAtom + 16;
+        // transform buffer (4 planes), two stages of the 3 input fields, the atom table
+        const size_t smem = sizeof(C) * (4 * M * PS + 6 * M * NZ) + sizeof(AtomPhase<T>) * a.z.in.nPhase * a.z.nAtom + 16;
         if (smem > max_smem(c)) return run_adj_z(c, a, st);
         QPD_TRY(set_smem(c, adj_zstage_fast<T, NZ, M, NT, RAD>, smem));
         const int64_t grid = (a.z.ncols + M - 1) / M;

@@ -519,7 +519,8 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
 // Adjoint z stage with a compile-time transform (the adj_zstage_kernel of qpd_kernels.cuh for the
 // lengths the forward specialises): per atom, the group's 3 conjugate adjoint fields times the z
 // factors become 4 pencils per column, transformed along z in shared memory; each cell then adds
-// its source transpose to dL/du and dL/dP held in registers.
+// its source transpose to dL/du and dL/dP held in registers.  The next atom's 3 fields arrive in a
+// second staging buffer by per-thread asynchronous copies while the current atom is transformed.
 // ---------------------------------------------------------------------------------------
 template <typename T, int NZ, int M, int NT, class RAD>
 __global__ void __launch_bounds__(NT, 2) adj_zstage_fast(AdjZArgs<T> a) {
@@ -531,8 +532,9 @@ __global__ void __launch_bounds__(NT, 2) adj_zstage_fast(AdjZArgs<T> a) {
     using GE = Geo<4 * M, 4 * M, PS, 0, 1, NT>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     C* buf = reinterpret_cast<C*>(smem_raw);
+    C* stg = buf + 4 * PLANE;  // 2 stages x 3 fields x CELLS: each thread's cells of one atom's fields
     const ZArgs<T>& z = a.z;
-    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(buf + 4 * PLANE);
+    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(stg + 6 * CELLS);
     const int tid = threadIdx.x;
     const int nap = z.in.nPhase * z.nAtom;
     for (int i = tid; i < nap; i += NT) apc[i] = z.apc[i];
@@ -558,9 +560,30 @@ __global__ void __launch_bounds__(NT, 2) adj_zstage_fast(AdjZArgs<T> a) {
             wt[q] = z.in.weight ? z.in.weight[g] : T(1);
         }
     }
+    // atom at's 3 fields at this thread's cells into stage sb (the thread later reads only these slots)
+    auto stage = [&](int at, int sb) {
+        const C* fa = a.fin + 3LL * z.grp[at] * z.fstride + g0;
+        C* d = stg + sb * 3 * CELLS;
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const int e = tid + q * NT;
+            if ((CELLS % NT == 0 || e < CELLS) && e < ncell) {
+                cp_async<sizeof(C)>(d + e, fa + e);
+                cp_async<sizeof(C)>(d + CELLS + e, fa + z.fstride + e);
+                cp_async<sizeof(C)>(d + 2 * CELLS + e, fa + 2 * z.fstride + e);
+            }
+        }
+        cp_async_commit();
+    };
+    if (z.nAtom > 0) stage(0, 0);
     __syncthreads();
     for (int at = 0; at < z.nAtom; at++) {
-        const C* fa = a.fin + 3LL * z.grp[at] * z.fstride + g0;
+        // the next atom's copies go into the other stage (last read two barriers ago); an empty group
+        // after the last atom keeps the count, so waiting for all but one group is atom at's data
+        if (at + 1 < z.nAtom) stage(at + 1, (at + 1) & 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        const C* sa = stg + (at & 1) * 3 * CELLS;
         const C* ce = z.coefE + (long long)at * NZ;
         const C* cu = z.coefUz + (long long)at * NZ;
 #pragma unroll
@@ -570,7 +593,7 @@ __global__ void __launch_bounds__(NT, 2) adj_zstage_fast(AdjZArgs<T> a) {
                 const int m = e / NZ;
                 const int kz = e - m * NZ;
                 const int s = m * PS + kz;
-                const C A = fa[e], X = fa[z.fstride + e], Y = fa[2 * z.fstride + e];
+                const C A = sa[e], X = sa[CELLS + e], Y = sa[2 * CELLS + e];
                 const C e1 = ce[kz], u1 = cu[kz];
                 buf[s] = cmul(e1, A);
                 buf[PLANE + s] = cmul(e1, X);
@@ -593,6 +616,7 @@ __global__ void __launch_bounds__(NT, 2) adj_zstage_fast(AdjZArgs<T> a) {
         }
         __syncthreads();
     }
+    cp_async_wait<0>();
 #pragma unroll
     for (int q = 0; q < CPT; q++) {
         const int e = tid + q * NT;
