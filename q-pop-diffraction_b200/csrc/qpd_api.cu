@@ -106,6 +106,10 @@ struct qpd_ctx {
     // the z stage's fields with y fastest so the 4000-point y transforms read contiguous pencils)
     int knob_yfast = 1;
     int knob_bulk_nt = 256;
+    // QPOP_B200_ZREGIN=0: nz = 64 and 128 z stages with 512 threads reading their inputs from shared
+    // memory for every atom, instead of 256 threads holding them in registers (0.262 against 0.239 ms
+    // at 256x256x64, 0.156 against 0.142 ms at 128^3)
+    int knob_zregin = 1;
     // QPOP_B200_ADJ_TMA=0: the adjoint's x and y passes on the generic kernels instead of the TMA one
     int knob_adj_tma = 1;  // QPOP_B200_BULK_NT: threads of the bulk y pass (256: 72.8 ms, 512: 80.9 ms)
     // QPOP_B200_OOP=0: in-place stages for the 256- and 512-point TMA passes (out-of-place measured
@@ -824,7 +828,9 @@ template <typename T> struct Impl {
         if (c->tma && ZLayout<T, 128, 8>::bytes(a.in.nPhase * a.nAtom, a.nAtom) <= max_smem(c)) {
             switch (a.nz) {
                 case 32: return smem_z_<32, F ? 32 : 16, F ? 512 : 256, Radix<8, 4>>(c, a, st);
-                case 64: return smem_z_<64, F ? 16 : 8, F ? 512 : 256, Radix<8, 8>>(c, a, st);
+                case 64:
+                    if (F && c->knob_zregin == 1) return smem_z_<64, 16, 256, Radix<8, 8>, true>(c, a, st);
+                    return smem_z_<64, F ? 16 : 8, F ? 512 : 256, Radix<8, 8>>(c, a, st);
                 case 68: return smem_z_<68, F ? 12 : 6, F ? 416 : 224, Pfa<4, 17>>(c, a, st);
                 case 104:
                     // float: 256 threads with each thread's inputs in registers measured fastest (1.82 ms at
@@ -832,7 +838,9 @@ template <typename T> struct Impl {
                     if (F && c->knob_z == 1) return smem_z_<104, 8, 416, Pfa<8, 13>>(c, a, st);
                     if (F) return smem_z_<104, 8, 256, Pfa<8, 13>, true>(c, a, st);
                     return smem_z_<104, 4, 224, Pfa<8, 13>>(c, a, st);
-                case 128: return smem_z_<128, F ? 8 : 4, F ? 512 : 256, Radix<8, 4, 4>>(c, a, st);
+                case 128:
+                    if (F && c->knob_zregin == 1) return smem_z_<128, 8, 256, Radix<8, 4, 4>, true>(c, a, st);
+                    return smem_z_<128, F ? 8 : 4, F ? 512 : 256, Radix<8, 4, 4>>(c, a, st);
             }
         }
         switch (a.nz) {
@@ -1605,6 +1613,7 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     if (const char* k = std::getenv("QPOP_B200_OOP")) c->knob_oop = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_YFAST")) c->knob_yfast = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_ADJ_TMA")) c->knob_adj_tma = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_ZREGIN")) c->knob_zregin = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_BULK_NT")) c->knob_bulk_nt = std::atoi(k) == 512 ? 512 : 256;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
