@@ -201,17 +201,20 @@ QPD_API int qpd_rsm_project(const double* I, int64_t nx, int64_t ny, int64_t nz,
 #define QPD_NOALLOC_SCRATCH_BYTES (32u << 20)
 
 /* No counterpart in the reference: an allocation-free variant of qpd_run_device for callers
- * that must not let a library allocate device memory (a stream being captured into a graph, a
- * framework whose allocator owns the GPU's memory, a real-time loop that reserves everything at
- * start-up).  Same float32 fused computation and the same caller-owned packed inputs (single
- * phase mode: phase index and optional weight) and output as qpd_run_device, but no context: the
- * grid and crystal come with the call, and the intermediate fields and tables live in one
- * library-wide device array of QPD_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
- * until exit.  Grids whose fields (96 bytes per cell for the perovskite cell) and tables do not fit
- * are refused with QPD_ERR_NOMEM; nAtom <= 16, nz <= 1024, nx, ny <= 4096.  The first call on a
- * device looks up the array's address, so make it before any stream capture.  Calls share the
- * array: calls that can overlap on the GPU race and must be serialised by the caller.  Failures
- * are described by qpd_last_error(NULL).  Asynchronous on `stream` (NULL: the default stream). */
+ * that must not let a library allocate device memory (a framework whose allocator owns the GPU's
+ * memory, a real-time loop that reserves everything at start-up).  Same float32 fused computation
+ * and the same caller-owned packed inputs (single phase mode: phase index and optional weight) and
+ * output as qpd_run_device, but no context: the grid and crystal come with the call, and the
+ * intermediate fields and tables live in one library-wide device array of
+ * QPD_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.  Grids whose
+ * fields (96 bytes per cell for the perovskite cell) and tables do not fit are refused with
+ * QPD_ERR_NOMEM; more than 12 distinct R_x, or more than 12 distinct R_y sharing one R_x, with
+ * QPD_ERR_UNSUPPORTED; both before anything is launched.  nAtom <= 16, nz <= 1024, nx, ny <= 4096.
+ * The first call on a device looks up the array's address and uploads constant tables with that
+ * device current, so make it before any stream capture; a device reset after it is not supported.
+ * Calls share the array: calls that can overlap on the GPU race and must be serialised by the
+ * caller.  Failures are described by qpd_last_error(NULL).  Asynchronous on `stream` (NULL: the
+ * default stream). */
 QPD_API int qpd_run_device_noalloc(const qpd_grid* grid, const qpd_crystal* crystal, const void* P, const void* U,
                                    const int8_t* phase, const void* weight, double* I_dev, void* stream);
 

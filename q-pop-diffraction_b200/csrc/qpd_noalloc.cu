@@ -1,19 +1,24 @@
 // qpd_run_device_noalloc: the fused float32 diffraction volume without any device allocation.
 //
-// Some callers cannot let a library call cudaMalloc: code that runs while a CUDA stream is being
-// captured into a graph, or under a framework whose caching allocator already owns the GPU's
-// memory and hands out buffers itself, or a real-time loop that reserves all of its memory at
-// start-up because an allocation can block the host and fail mid-run.  For them this entry point
-// keeps every intermediate (the folded z-stage fields, twiddles, phase tables and segment
-// descriptors) in one file-scope device array, g_noalloc_scratch, of QPD_NOALLOC_SCRATCH_BYTES.
-// The caller supplies the packed inputs and the output buffer, exactly as for qpd_run_device.
+// Some callers cannot let a library call cudaMalloc: a framework whose caching allocator already
+// owns the GPU's memory and hands out buffers itself, or a real-time loop that reserves all of its
+// memory at start-up because an allocation can block the host and fail mid-run.  For them this
+// entry point keeps every intermediate (the folded z-stage fields, twiddles, phase tables and
+// segment descriptors) in one file-scope device array, g_noalloc_scratch, of
+// QPD_NOALLOC_SCRATCH_BYTES.  The caller supplies the packed inputs and the output buffer, exactly
+// as for qpd_run_device.
 //
 // Costs and limits: every GPU that loads the library holds the array until the process exits;
-// grids whose fields and tables do not fit are refused with QPD_ERR_NOMEM before any launch.
+// grids whose fields and tables do not fit are refused with QPD_ERR_NOMEM, and crystals with more
+// atom groups than the fused passes' segments hold with QPD_ERR_UNSUPPORTED, before any launch.
 // All calls share the one array and each call overwrites it: calls that may overlap on the GPU
-// (other streams, other host threads) race and must be serialised by the caller.  The array's
-// device address is looked up once per device, on that device's first call (cudaGetSymbolAddress);
-// make that first call before any stream capture.
+// (other streams, other host threads) race and must be serialised by the caller.  The first call
+// on a device looks up the array's device address (cudaGetSymbolAddress) and uploads the
+// butterflies' unit roots to constant memory, with that device current; make that first call
+// before any stream capture.  Both are cached per device ordinal for the life of the process, so a
+// device reset (cudaDeviceReset) after the first call is not supported.  The per-call constants
+// and segment descriptors travel as a kernel argument, so no host memory is read after the call
+// returns.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,6 +40,8 @@ namespace {
 constexpr size_t kNoAllocBytes = (size_t)QPD_NOALLOC_SCRATCH_BYTES;
 constexpr int kNoAllocAtoms = 16;
 constexpr int kNoAllocGroups = kNoAllocAtoms;
+constexpr int kNoAllocApc = 64;                // nAtom * nPhase
+constexpr int kNoAllocSegs = kMaxSegIn + 1;    // 2 G2 y-pass segments (2 G2 <= kMaxSegIn) + the x pass
 constexpr int kMaxDevices = 64;
 
 int nfail(int code, const char* msg) {
@@ -189,6 +196,20 @@ __global__ void noalloc_tables(TableJob j) {
     }
 }
 
+// Per-call constants and segment descriptors: one kernel argument (under the 32 KB parameter limit),
+// copied into the scratch array by noalloc_upload.
+struct Upload {
+    AtomPhase<float> apc[kNoAllocApc];
+    Segment<float> seg[kNoAllocSegs];
+    int napc, nseg;
+};
+static_assert(sizeof(Upload) < 32000, "the upload must fit the kernel parameter space");
+
+__global__ void noalloc_upload(const __grid_constant__ Upload u, AtomPhase<float>* apc, Segment<float>* seg) {
+    for (int i = threadIdx.x; i < u.napc; i += blockDim.x) apc[i] = u.apc[i];
+    for (int i = threadIdx.x; i < u.nseg; i += blockDim.x) seg[i] = u.seg[i];
+}
+
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 }  // namespace
@@ -202,7 +223,8 @@ extern "C" int qpd_run_device_noalloc(const qpd_grid* grid, const qpd_crystal* k
     if (k->nAtom < 1 || k->nAtom > kNoAllocAtoms) return nfail(QPD_ERR_ARG, "nAtom outside 1..16 for the allocation-free call");
     if (k->nPhase < 1 || k->nPhase > kMaxPhases || k->nStruc < 0 || k->nStruc > 3)
         return nfail(QPD_ERR_ARG, "nPhase outside 1..8 or nStruc outside 0..3");
-    if (k->nAtom * k->nPhase > 64) return nfail(QPD_ERR_ARG, "nAtom * nPhase above 64 for the allocation-free call");
+    if (k->nAtom * k->nPhase > kNoAllocApc)
+        return nfail(QPD_ERR_ARG, "nAtom * nPhase above 64 for the allocation-free call");
     if (!k->R || !k->f_re || !k->f_im || (k->nStruc > 0 && !k->su)) return nfail(QPD_ERR_ARG, "crystal arrays are NULL");
     if (nz > 1024 || nx > 4096 || ny > 4096) return nfail(QPD_ERR_UNSUPPORTED, "the allocation-free call takes nz <= 1024, nx, ny <= 4096");
     const int A = k->nAtom, NP = k->nPhase, NS = k->nStruc;
@@ -242,6 +264,15 @@ extern "C" int qpd_run_device_noalloc(const qpd_grid* grid, const qpd_crystal* k
     for (int g = 0; g < G1; g++)
         for (int a = 0; a < A; a++)
             if (g1a[a] == g) order[no++] = a;
+    // segment limits of the fused passes, checked before anything is launched: the x pass reads
+    // 2 fields per R_x group, a y-pass segment 2 fields per (R_x, R_y) group sharing its R_x
+    if (2 * G2 > kMaxSegIn) return nfail(QPD_ERR_UNSUPPORTED, "more than 12 distinct R_x for the allocation-free call");
+    for (int g2 = 0; g2 < G2; g2++) {
+        int cnt = 0;
+        for (int g1 = 0; g1 < G1; g1++) cnt += g2of[g1] == g2;
+        if (2 * cnt > kMaxSegIn)
+            return nfail(QPD_ERR_UNSUPPORTED, "more than 12 distinct R_y share one R_x for the allocation-free call");
+    }
 
     // scratch layout
     size_t off = 0;
@@ -295,9 +326,10 @@ extern "C" int qpd_run_device_noalloc(const qpd_grid* grid, const qpd_crystal* k
     noalloc_tables<<<148, 256, 0, st>>>(tj);
     NA_CU(cudaGetLastError());
 
-    // per (phase, atom) constants and segment descriptors, assembled on the host stack
-    AtomPhase<float> apc[64];
-    std::memset(apc, 0, sizeof apc);
+    // per (phase, atom) constants and segment descriptors, passed to the device by value
+    Upload up;
+    std::memset(&up, 0, sizeof up);
+    AtomPhase<float>* apc = up.apc;
     for (int p = 0; p < NP; p++)
         for (int i = 0; i < A; i++) {
             const int a = order[i];
@@ -314,8 +346,7 @@ extern "C" int qpd_run_device_noalloc(const qpd_grid* grid, const qpd_crystal* k
             e.fr = (float)k->f_re[p * A + a];
             e.fi = (float)k->f_im[p * A + a];
         }
-    Segment<float> seg[2 * kNoAllocGroups + 1];
-    std::memset(seg, 0, sizeof seg);
+    Segment<float>* seg = up.seg;
     const float2* ytab = tj.ytab;
     const float2* xtab = tj.xtab;
     int s = 0;
@@ -325,7 +356,6 @@ extern "C" int qpd_run_device_noalloc(const qpd_grid* grid, const qpd_crystal* k
             seg[s].out[0] = 2 * g2 + out;
             for (int g1 = 0; g1 < G1; g1++) {
                 if (g2of[g1] != g2) continue;
-                if (seg[s].nin + 2 > kMaxSegIn) return nfail(QPD_ERR_UNSUPPORTED, "too many atom groups share one R_x");
                 if (out == 0) {
                     seg[s].in[seg[s].nin] = 3 * g1;
                     seg[s].coef[0][seg[s].nin++] = ytab + (2 * g1) * ny;
@@ -344,9 +374,11 @@ extern "C" int qpd_run_device_noalloc(const qpd_grid* grid, const qpd_crystal* k
         seg[s].in[seg[s].nin] = 2 * g2 + 1;
         seg[s].coef[0][seg[s].nin++] = xtab + (2 * g2 + 1) * nx;
     }
-    // pageable host sources: the copies are staged before the calls return, so the stack arrays may go
-    NA_CU(cudaMemcpyAsync(base + o_apc, apc, sizeof(AtomPhase<float>) * NP * A, cudaMemcpyHostToDevice, st));
-    NA_CU(cudaMemcpyAsync(base + o_seg, seg, sizeof(Segment<float>) * nseg, cudaMemcpyHostToDevice, st));
+    up.napc = NP * A;
+    up.nseg = nseg;
+    noalloc_upload<<<1, 128, 0, st>>>(up, reinterpret_cast<AtomPhase<float>*>(base + o_apc),
+                                      reinterpret_cast<Segment<float>*>(base + o_seg));
+    NA_CU(cudaGetLastError());
 
     Inputs<float> in;
     in.P = static_cast<const float*>(P);

@@ -1,13 +1,12 @@
 """
 Python binding of qpd_run_device_noalloc, the allocation-free variant of the device path.
 
-It is for callers that must not let a library allocate GPU memory: work recorded while a CUDA
-stream is captured into a graph, a framework whose caching allocator owns the device's memory,
-or a real-time loop that reserves all of its memory up front.  The float32 fused computation is
+It is for callers that must not let a library allocate GPU memory: a framework whose caching
+allocator owns the device's memory, or a real-time loop that reserves all of its memory up front.  The float32 fused computation is
 the same as ``Plan.run_device``; the intermediate fields and tables live in one fixed device
 array inside the library (``QPD_NOALLOC_SCRATCH_BYTES``, 32 MiB, held by every GPU that loads
 the library until the process exits), so only small grids fit and larger ones are refused with
-a MemoryError.  All calls share that array: calls that can overlap on the GPU race, so the
+a MemoryError; crystals with more than 12 distinct R_x are refused with a ValueError.  All calls share that array: calls that can overlap on the GPU race, so the
 caller serialises them.  The first call on a device looks up the array's address; make it
 before any stream capture.
 """
