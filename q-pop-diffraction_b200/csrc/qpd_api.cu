@@ -22,6 +22,7 @@
 #include "qpd_zpfa.cuh"
 #include "qpd_host.h"
 #include "qpd_kernels.cuh"
+#include "qpd_n4000.h"
 
 using namespace qpd;
 
@@ -67,6 +68,10 @@ struct qpd_ctx {
     int nsegY = 0;
     size_t off_segAX = 0, off_segAY = 0;  // adjoint passes
     int nsegAX = 0, nsegAY = 0;
+    // register-resident 4000-point passes (float32 fused): their input descriptors, device addresses
+    // inside `tables` (have_p4y: ny = 4000, have_p4x: nx = 4000)
+    bool have_p4y = false, have_p4x = false;
+    qpd::Pass4k p4y, p4x;
 
     // workspace
     DevMem fields;  // fused: 3 * ng1 fields; plain: buf + amp
@@ -112,6 +117,9 @@ struct qpd_ctx {
     int knob_zregin = 1;
     // QPOP_B200_ADJ_TMA=0: the adjoint's x and y passes on the generic kernels instead of the TMA one
     int knob_adj_tma = 1;  // QPOP_B200_BULK_NT: threads of the bulk y pass (256: 72.8 ms, 512: 80.9 ms)
+    // QPOP_B200_N4K=0: the 4000-point passes on the shared-memory Stockham kernels (axis_tma, axis_bulk)
+    // instead of the register-resident ones of qpd_n4000.cu
+    int knob_n4k = 1;
     // QPOP_B200_OOP=0: in-place stages for the 256- and 512-point TMA passes (out-of-place measured
     // 1.080 against 1.104 ms for the y pass at 512x512x104)
     int knob_oop = 1;
@@ -419,6 +427,11 @@ template <typename T> struct Impl {
             std::memcpy(host.data() + c->off_S[d], S[d].data(), sizeof(double) * N[d]);
         }
         std::vector<Segment<T>> segY, segX, segAX, segAY;
+        // inputs of the register-resident 4000-point y pass, in segment order: field, g1, -i k_y, closes a
+        // segment, its output field
+        size_t off4y = 0, off4x = 0;
+        std::vector<int> in4y_g, in4y_ik, in4y_f, in4y_last, in4y_out;
+        const bool f4y = sizeof(T) == 4 && N[1] == 4000, f4x = sizeof(T) == 4 && N[0] == 4000;
         if (sched == QPD_SCHED_FUSED) {
             c->off_coefE = place(sizeof(C) * A * N[2]);
             c->off_coefUz = place(sizeof(C) * A * N[2]);
@@ -452,6 +465,26 @@ template <typename T> struct Impl {
                     t[N[0] + x] = to_c<T>(make_double2(kd[0][x] * e.y, -kd[0][x] * e.x));
                 }
             }
+            // fold factors of the register-resident 4000-point passes (float32): per g1 for a 4000-point y
+            // axis, per g2 for a 4000-point x axis, 200 values u[t] then 20 values V[r] each (Pass4k)
+            auto fold4k = [&](C* dst, int64_t Nd, double hd, double G, double Rd) {
+                const double val = 1.0 / ((double)Nd * hd);
+                for (int t = 0; t < 200; t++) dst[t] = to_c<T>(expmi(2.0 * M_PI * ((double)t * val) * Rd));
+                for (int r = 0; r < 20; r++) {
+                    const double m = 200.0 * r - (r >= 10 ? (double)Nd : 0.0);
+                    dst[200 + r] = to_c<T>(expmi(2.0 * M_PI * (m * val) * Rd + G * Rd));
+                }
+            };
+            if (f4y) {
+                off4y = place(sizeof(C) * 220 * G1);
+                for (int g1 = 0; g1 < G1; g1++)
+                    fold4k(reinterpret_cast<C*>(host.data() + off4y) + 220 * g1, N[1], c->h[1], k->G[1], ry[g1]);
+            }
+            if (f4x) {
+                off4x = place(sizeof(C) * 220 * G2);
+                for (int g2 = 0; g2 < G2; g2++)
+                    fold4k(reinterpret_cast<C*>(host.data() + off4x) + 220 * g2, N[0], c->h[0], k->G[0], rx[g2]);
+            }
             // segments hold device addresses: filled in once the buffer exists
             // one output per segment: E2 <- (E1, Y1) of the g1 groups sharing R_x, then X2 <- X1.
             // Writing E2 into slot 2 g2 before X1 of the same g2 is read is safe: X1 slots are 3 g1 + 1 > 2 g2.
@@ -470,10 +503,22 @@ template <typename T> struct Impl {
                             s.coef[0][s.nin++] = reinterpret_cast<const C*>(e);
                             s.in[s.nin] = 3 * g1 + 2;
                             s.coef[0][s.nin++] = reinterpret_cast<const C*>(mi);
+                            in4y_f.insert(in4y_f.end(), {3 * g1, 3 * g1 + 2});
+                            in4y_g.insert(in4y_g.end(), {g1, g1});
+                            in4y_ik.insert(in4y_ik.end(), {0, 1});
                         } else {
                             s.in[s.nin] = 3 * g1 + 1;
                             s.coef[0][s.nin++] = reinterpret_cast<const C*>(e);
+                            in4y_f.push_back(3 * g1 + 1);
+                            in4y_g.push_back(g1);
+                            in4y_ik.push_back(0);
                         }
+                    }
+                    in4y_last.resize(in4y_f.size(), 0);
+                    in4y_out.resize(in4y_f.size(), 0);
+                    if (!in4y_f.empty()) {
+                        in4y_last.back() = 1;
+                        in4y_out.back() = 2 * g2 + out;
                     }
                     segY.push_back(s);
                 }
@@ -548,6 +593,41 @@ template <typename T> struct Impl {
                     if (s.coef[o][i]) s.coef[o][i] = reinterpret_cast<const C*>(base + reinterpret_cast<uintptr_t>(s.coef[o][i]) - 1);
         };
         for (auto& s : segY) fix(s);
+        c->have_p4y = c->have_p4x = false;
+        if constexpr (sizeof(T) == 4) {
+            if (sched == QPD_SCHED_FUSED && f4y && (int)in4y_f.size() <= kPass4kMax) {
+                Pass4k& P = c->p4y;
+                std::memset(&P, 0, sizeof P);
+                for (size_t i = 0; i < in4y_f.size(); i++) {
+                    const C* u = reinterpret_cast<const C*>(base + off4y) + 220 * in4y_g[i];
+                    P.u[P.n] = u;
+                    P.V[P.n] = u + 200;
+                    P.field[P.n] = in4y_f[i];
+                    P.out[P.n] = in4y_out[i];
+                    if (in4y_ik[i]) P.ik |= 1ull << P.n;
+                    if (in4y_last[i]) P.last |= 1ull << P.n;
+                    P.n++;
+                }
+                P.kscale = (float)(2.0 * M_PI * (1.0 / ((double)c->ny * c->h[1])));
+                c->have_p4y = true;
+            }
+            if (sched == QPD_SCHED_FUSED && f4x && 2 * G2 <= kPass4kMax) {
+                Pass4k& P = c->p4x;
+                std::memset(&P, 0, sizeof P);
+                for (int g2 = 0; g2 < G2; g2++)
+                    for (int kind = 0; kind < 2; kind++) {
+                        const C* u = reinterpret_cast<const C*>(base + off4x) + 220 * g2;
+                        P.u[P.n] = u;
+                        P.V[P.n] = u + 200;
+                        P.field[P.n] = 2 * g2 + kind;
+                        if (kind) P.ik |= 1ull << P.n;
+                        P.n++;
+                    }
+                P.last = 1ull << (P.n - 1);
+                P.kscale = (float)(2.0 * M_PI * (1.0 / ((double)c->nx * c->h[0])));
+                c->have_p4x = true;
+            }
+        }
         for (auto& s : segX) fix(s);
         for (auto& s : segAX) fix(s);
         for (auto& s : segAY) fix(s);
@@ -920,6 +1000,10 @@ template <typename T> struct Impl {
                ZPfaLayout<T, 4, 17>::bytes(in.nPhase * c->nAtom, c->nAtom) <= max_smem(c);
     }
 
+    // The y-fastest route on the register-resident passes: (k_z, x, y) fields, bulk y pass, strided x pass
+    // (the shared-memory Stockham passes read the (x, k_z, y) layout instead).
+    static bool yfast4k(const qpd_ctx* c) { return c->knob_n4k && c->have_p4y && c->have_p4x; }
+
     // float: z chunks of 8 complex64 (64-byte rows), 16-byte accesses when nz is even;
     // double: chunks of 4 complex128 (64-byte rows).
     template <int N, int NT, bool EPI, class RAD>
@@ -955,6 +1039,22 @@ template <typename T> struct Impl {
             case 512: return fast_axis_n<512, 512, EPI, Radix<8, 8, 8>>(c, a, nouter, kind, st);
             case 1024: return fast_axis_n<1024, 1024, EPI, Radix<8, 8, 4, 4>>(c, a, nouter, kind, st);
             case 4000:
+                if constexpr (sizeof(T) == 4) {
+                    const bool yp = kind == QPD_K_YPASS && c->have_p4y, xp4 = kind == QPD_K_XPASS && c->have_p4x;
+                    if (c->knob_n4k && c->tma && a.nz % 2 == 0 && !a.accumulate && (yp || xp4)) {
+                        // register-resident passes over tiles of two neighbouring z values: rows along y for the y
+                        // pass, along x for the x pass
+                        CUtensorMap map;
+                        const int64_t nfields = 3 * c->ng1;
+                        QPD_TRY(field_map(c, &map, const_cast<C*>(a.in), false, c->nz, c->ny, nfields * c->nx, 4,
+                                          yp ? 200 : 1, yp ? 1 : 200));
+                        cudaEvent_t t0;
+                        QPD_TRY(tstart(c, st, &t0));
+                        QPD_CU(c, launch_strided4000(map, a, yp ? c->p4y : c->p4x, (int)nouter,
+                                                     yp ? Strided4k::YPassZFast : Strided4k::XPassZFast, st));
+                        return tstop(c, kind, st, t0);
+                    }
+                }
                 // 4000 x 2 tiles (16-byte rows: the other half of each 32-byte sector is read by the CTA of
                 // the neighbouring z chunk while it is still in L2), 200-row boxes, two buffers
                 if constexpr (sizeof(T) == 4) {
@@ -1131,7 +1231,7 @@ template <typename T> struct Impl {
             bool done = false;
             if constexpr (sizeof(T) == 4) {
                 if (yfast) {
-                    z.yfast = 1;
+                    z.yfast = yfast4k(c) ? 2 : 1;
                     z.ny = c->ny;
                     QPD_TRY((pfa_z_<4, 17>(c, z, st)));
                     done = true;
@@ -1157,6 +1257,12 @@ template <typename T> struct Impl {
             y.status = static_cast<int*>(c->status.p);
             if (yfast) {
                 if constexpr (sizeof(T) == 4) {
+                    if (yfast4k(c)) {
+                        cudaEvent_t t0;
+                        QPD_TRY(tstart(c, st, &t0));
+                        QPD_CU(c, launch_ypass4000(y, c->p4y, c->nx * c->nz, st));
+                        return tstop(c, QPD_K_YPASS, st, t0);
+                    }
                     if (c->knob_bulk_nt == 512) return bulk_axis_<4000, 512, Radix<8, 4, 5, 5, 5>>(c, y, st);
                     return bulk_axis_<4000, 256, Radix<8, 4, 5, 5, 5>>(c, y, st);
                 }
@@ -1179,6 +1285,16 @@ template <typename T> struct Impl {
             if constexpr (sizeof(T) == 4) {
                 if (yfast) {
                     x.nz = (int)c->ny;  // the contiguous axis of the y-fastest fields
+                    if (yfast4k(c)) {
+                        // (k_z, x, y) fields: tiles of two neighbouring k_y at one k_z, rows along x (ny values apart)
+                        CUtensorMap map;
+                        QPD_TRY(field_map(c, &map, const_cast<C*>(x.in), false, c->ny, c->nx, 3 * c->ng1 * c->nz, 4, 200,
+                                          1));
+                        cudaEvent_t t0;
+                        QPD_TRY(tstart(c, st, &t0));
+                        QPD_CU(c, launch_strided4000(map, x, c->p4x, (int)c->nz, Strided4k::XPassYFast, st));
+                        return tstop(c, QPD_K_XPASS, st, t0);
+                    }
                     return tma_axis_b<4000, 2, 512, 2, true, true, Radix<8, 4, 5, 5, 5>, 2, true, true>(c, x, c->nz,
                                                                                                     QPD_K_XPASS, st);
                 }
@@ -1612,6 +1728,7 @@ int qpd_create(int device, uint64_t hbm_budget_bytes, qpd_ctx** out) {
     if (const char* k = std::getenv("QPOP_B200_N4000")) c->knob_n4000 = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_OOP")) c->knob_oop = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_YFAST")) c->knob_yfast = std::atoi(k);
+    if (const char* k = std::getenv("QPOP_B200_N4K")) c->knob_n4k = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_ADJ_TMA")) c->knob_adj_tma = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_ZREGIN")) c->knob_zregin = std::atoi(k);
     if (const char* k = std::getenv("QPOP_B200_BULK_NT")) c->knob_bulk_nt = std::atoi(k) == 512 ? 512 : 256;

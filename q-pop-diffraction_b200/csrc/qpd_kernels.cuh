@@ -181,7 +181,7 @@ template <typename T> struct ZArgs {
     AxisPlan zp;
     int* status;                  // device status word: bounded waits record timeouts here
     long long ny;                 // yfast: the y extent
-    int yfast;                    // 1: fields laid out (x, k_z, y), y fastest (zstage_pfa only)
+    int yfast;                    // fields y fastest (zstage_pfa only): 1 (x, k_z, y), 2 (k_z, x, y)
 };
 
 template <typename T, int NT, int EPT>

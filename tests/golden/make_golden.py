@@ -11,7 +11,7 @@ CPU (QPOP_DIFFRACTION_DEVICE=cpu, as src/python/diffraction.py:24-33 reads it).
 
 Run from the repository root, in a container where the reference is mounted:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference]   (default: QPOP_REFERENCE_ROOT, else ../reference)
 
 Each fixture ``<name>.npz`` holds the grid, the crystal, the inputs (float32
 values; or, for the larger config-1 case, SHA-256 digests of the regenerated
@@ -28,6 +28,9 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import reference_pkg  # noqa: E402
 
 from qpop_diffraction_b200 import workloads  # noqa: E402
 
@@ -62,7 +65,9 @@ def cases():
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else reference_pkg.source_root()
+    if ref_root is None:
+        sys.exit("give the reference's source checkout as the argument or in QPOP_REFERENCE_ROOT")
     diffraction = load_reference(ref_root)
     for case, store_inputs in cases():
         I, qx, qy, qz = diffraction(*case.args())

@@ -14,7 +14,7 @@ from the reference through a package shim, as make_golden.py does) and reading t
 with qpop_diffraction_b200.hdf5.  It stores them, the legacy intensity and the reference's own
 diffraction() result in tests/golden/polar_vortex_example.npz.
 
-    python tests/golden/make_legacy_case.py [/path/to/reference]
+    python tests/golden/make_legacy_case.py [/path/to/reference]   (default: QPOP_REFERENCE_ROOT, else ../reference)
 """
 
 import sys
@@ -25,6 +25,9 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import reference_pkg  # noqa: E402
 
 from qpop_diffraction_b200 import hdf5  # noqa: E402
 
@@ -50,7 +53,9 @@ def field(path, name):
 
 
 def main():
-    ref_root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref_root = Path(sys.argv[1]) if len(sys.argv) > 1 else reference_pkg.source_root()
+    if ref_root is None:
+        sys.exit("give the reference's source checkout as the argument or in QPOP_REFERENCE_ROOT")
     SizeContext, AtomList, diffraction = load_reference(ref_root)
     case = ref_root / CASE
     params = SizeContext()

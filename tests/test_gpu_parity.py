@@ -226,8 +226,11 @@ def test_prime_factor_z_stage_equals_stockham(gpu, monkeypatch, shape, weights):
 
 def test_y_fastest_route_at_4000x4000x68(gpu, monkeypatch):
     """The 4000 x 4000 x 68 route (z stage writing y-fastest fields, bulk y pass, swapped x pass)
-    against the z-fastest route of the same kernels, on the full config-3 volume."""
+    against the z-fastest route of the same kernels, on the full config-3 volume, with the
+    shared-memory Stockham 4000-point passes (QPOP_B200_N4K=0), whose two routes round differently.
+    The register-resident passes compute both routes with the same arithmetic (tested below)."""
     torch = gpu
+    monkeypatch.setenv("QPOP_B200_N4K", "0")
     torch.cuda.empty_cache()  # blocks an earlier test left in the caching allocator
     free, _ = torch.cuda.mem_get_info(0)
     if free < 160e9:
@@ -252,6 +255,46 @@ def test_y_fastest_route_at_4000x4000x68(gpu, monkeypatch):
             # the routes round differently (two-level twiddles in the bulk y pass): identical bits would
             # mean the y-fastest route did not run
             assert not torch.equal(out, ref)
+
+
+def test_register_4000_point_passes_at_4000x4000x68(gpu, monkeypatch):
+    """The register-resident 4000-point y and x passes (qpd_n4000.cu, the default) against the
+    shared-memory Stockham passes (QPOP_B200_N4K=0) on the full config-3 volume."""
+    torch = gpu
+    torch.cuda.empty_cache()  # blocks an earlier test left in the caching allocator
+    free, _ = torch.cuda.mem_get_info(0)
+    if free < 160e9:
+        pytest.skip("needs about 150 GB of free device memory")
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    shape = (4000, 4000, 68)
+    params, inputs = workloads.gpu_snapshot("twin", shape, seed=3, device="cuda:0", n_phase=1)
+    crystal = crystal_from(params, workloads.config3_crystal(3, (1, 1, 3)))
+    out = torch.empty(shape, dtype=torch.float64, device="cuda:0")
+    for knob in ("0", "1"):
+        monkeypatch.setenv("QPOP_B200_N4K", knob)
+        with Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp32") as plan:
+            plan.set_crystal(crystal)
+            plan.run_device(inputs, out)
+            torch.cuda.synchronize()
+            plan.device_status()
+        if knob == "0":
+            ref = out.clone()
+        else:
+            dmax = ((out - ref).abs().max() / ref.max()).item()
+            assert dmax <= 1e-6, dmax
+            # different twiddle and butterfly rounding: identical bits would mean the new passes did not run
+            assert not torch.equal(out, ref)
+    # with the register-resident passes the z-fastest route (strided y pass) gives the same bits as the
+    # y-fastest one (bulk y pass): the same transforms and folds in the same order
+    monkeypatch.setenv("QPOP_B200_N4K", "1")
+    for knob, dst in (("0", ref), ("1", out)):
+        monkeypatch.setenv("QPOP_B200_YFAST", knob)
+        with Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp32") as plan:
+            plan.set_crystal(crystal)
+            plan.run_device(inputs, dst)
+            torch.cuda.synchronize()
+            plan.device_status()
+    assert torch.equal(out, ref)
 
 
 def test_direct_sum_voxels_at_4000x4000x68(gpu):
