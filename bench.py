@@ -19,12 +19,18 @@ Printed (rank 0, one JSON line):
             float64 intensity copied back, all inside the timed region;
   roofline  the dominant kernel's algorithmic bytes per launch / its mean event-timed duration,
             against the measured HBM copy bandwidth;
-  cpu_baseline  the oracle (a NumPy restatement of the reference's diffraction()) on a bounded
-            sample of the same workload, on this host's cores;
+  cpu_baseline  the reference's own NumPy diffraction() (the unmodified package installed under
+            baseline/_ref) on the full 512 x 512 x 104 grid, one run on this host; its result is also
+            the float64 oracle of the full-grid accuracy figures;
   fp64      the same hand-written kernels in float64, fused and plain (the reference's own
-            per-atom, per-component schedule), for the float32-vs-float64 comparison.
+            per-atom, per-component schedule), for the float32-vs-float64 comparison;
+  config3   the 4000 x 4000 x 68 twin film on one GPU: per-pass times and roofline fractions,
+            device memory and float64 direct sums at 64 voxels (bench.py --config 3 adds one
+            end-to-end volume from float64 host arrays through qpd_run_host).
 
-With --impl reference only the CPU oracle runs (rank 0), on bounded samples of the workload.
+With --impl reference only the reference's own diffraction() runs (rank 0, NumPy with its own
+threading, as the reference computes), on a bounded crop of the workload per step; the oracle
+port stands in when baseline/_ref is absent.
 Under torchrun each rank evaluates its own volumes on its own GPU (replicas: the path has no
 cross-volume exchange), so scaling is weak.
 """
@@ -50,8 +56,7 @@ GRID = (512, 512, 104)
 REFLECTIONS = ((0, 0, 2), (1, 0, 3))
 METRIC = "Gcells/s per 3-D volume at 512x512x104 (float32 source+FFT, float64 phase reduction)"
 UNIT = "Gcells/s"
-CPU_SAMPLE = (256, 384, 104)        # cpu_baseline: a bounded sample, several seconds of NumPy work
-REF_SAMPLE = (64, 64, 104)          # --impl reference: one step, so K + W steps end in minutes
+REF_SAMPLE = (128, 128, 104)        # --impl reference: one step, so K + W steps end in minutes
 FALLBACK_HBM = 6650.0
 
 
@@ -71,6 +76,7 @@ def parse():
     ap.add_argument("--config", type=int, default=2, choices=(2, 3),
                     help="3: the 4000x4000x68 twin film on one GPU (device-resident, per-pass roofline)")
     ap.add_argument("--validate", action="store_true", help="with --config 3: compare against a float64 plain run")
+    ap.add_argument("--no-config3", action="store_true", help="skip the 4000x4000x68 leg of the default run")
     return ap.parse_args()
 
 
@@ -163,33 +169,65 @@ def profiled_traffic():
     return out
 
 
-def cpu_oracle_rate(shape, threads):
-    """Cells/s of the oracle (the reference's NumPy diffraction(), restated) on the config-2 snapshot."""
-    from oracle import diffraction_oracle as oracle
-    from qpop_diffraction_b200 import workloads
-    case = workloads.config2(shape=shape, hkl=REFLECTIONS[0])
-    t = time.perf_counter()
-    oracle.diffraction(*case.args(), threads=threads)
-    dt = time.perf_counter() - t
-    return case.params.n / dt, dt
+def host_cpu():
+    """CPU model and core count of this host."""
+    model = "unknown CPU"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{model}, {os.cpu_count()} cores"
+
+
+def reference_diffraction():
+    """
+    The reference's own diffraction() (baseline/_ref or a source checkout), or None.  Called with its
+    progress prints (G, qC) sent to /dev/null, so the JSON line stays the last line of the output.
+    """
+    import contextlib
+    sys.path.insert(0, str(ROOT / "tests"))
+    import reference_pkg
+    mods = reference_pkg.load("diffraction")
+    if mods is None:
+        return None
+    fn = mods[0].diffraction
+
+    def quiet(*a, **k):
+        with open(os.devnull, "w") as null, contextlib.redirect_stdout(null):
+            return fn(*a, **k)
+    return quiet
 
 
 def run_reference(args, rank):
+    """
+    The reference arm: the unmodified reference diffraction() (src/python/diffraction.py:62-113, NumPy
+    with its own threading, as the reference runs) on a crop of the config-2 snapshot, both reflections
+    alternating.
+    """
     if rank != 0:
         return
-    from oracle import diffraction_oracle as oracle
     from qpop_diffraction_b200 import workloads
-    threads = oracle.default_threads(5)
+    diffraction = reference_diffraction()
+    kind, cores = "reference", os.cpu_count()  # as the reference runs: NumPy's own threading
+    if diffraction is None:  # no install and no checkout: the oracle port, the same algorithm restated
+        from oracle import diffraction_oracle as oracle
+        diffraction, kind = oracle.diffraction, "port"
     cases = [workloads.config2(shape=REF_SAMPLE, hkl=h) for h in REFLECTIONS]
     for i in range(args.warmup):
-        oracle.diffraction(*cases[i % 2].args(), threads=threads)
+        diffraction(*cases[i % 2].args())
     t = time.perf_counter()
     for i in range(args.steps):
-        oracle.diffraction(*cases[i % 2].args(), threads=threads)
+        diffraction(*cases[i % 2].args())
     dt = time.perf_counter() - t
     n = cases[0].params.n
     value = args.steps * n / dt / 1e9
-    sample = f"config-2 snapshot cropped to {'x'.join(map(str, REF_SAMPLE))}, both reflections alternating"
+    who = "the reference's own diffraction() (baseline/_ref, unmodified, NumPy as installed)" if kind == "reference" else \
+          "the oracle port of the reference's diffraction() (NumPy)"
+    sample = (f"{who} on the config-2 snapshot cropped to {'x'.join(map(str, REF_SAMPLE))}, G=002,103 alternating, "
+              f"one crop per step; host {host_cpu()}")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -197,7 +235,7 @@ def run_reference(args, rank):
         "config": {"workload": f"two-phase polar-vortex film {'x'.join(map(str, GRID))}, 5 atoms, 2 phases, "
                                f"G=002,103 alternating", "grid": list(GRID), "cells": int(np.prod(GRID)), "atoms": 5,
                    "phases": 2, "precision": "fp64 (NumPy, as the reference computes)", "sample": sample},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -205,23 +243,43 @@ def run_reference(args, rank):
 CONFIG3 = (4000, 4000, 68)
 
 
-def run_config3(args, torch, dev, rank, world):
+def intensity_errors(I, ref):
+    """Float32-contract figures of I against a float64 reference volume (numpy or torch)."""
+    I = np.asarray(I, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    imax = ref.max()
+    strong = ref > 1e-6 * imax
+    dlog = np.abs(np.log10(I[strong]) - np.log10(ref[strong]))
+    return {"max_abs_dI_over_Imax": float(np.abs(I - ref).max() / imax),
+            "max_rel_err_above_1e-6_Imax": float((np.abs(I - ref)[strong] / ref[strong]).max()),
+            "max_abs_dlog10I_above_1e-6_Imax": float(dlog.max()),
+            "voxels_above_1e-6_Imax": int(strong.sum()),
+            "contract": "max |dI|/I_max <= 1e-5, rel <= 1e-3 above 1e-6 I_max"}
+
+
+def config3_leg(args, torch, dev, rank, world, shape=CONFIG3, steps=3, warmup=1, validate=False, direct=True,
+                e2e=True):
     """
     The 4000 x 4000 x 68 three-variant Voronoi twin film (1.09e9 cells, one phase, G = 113) on one
-    GPU: generated on the device, float32 fused schedule, inputs resident.  With --validate, the
-    same volume in float64 with the plain (per atom and component) schedule, compared on the GPU.
+    GPU: generated on the device, float32 fused schedule, inputs resident; per-pass event times.
+    direct: float64 direct sums over all cells at 64 voxels (32 brightest, 32 random) against the
+    volume (tests/direct_dft.py, no FFT).  e2e: one volume from float64 host arrays in the reference
+    layout through qpd_run_host (host arrays of about 78 GB), timed with its copies.  validate: the
+    same volume in float64 with the plain schedule, compared on the GPU.
     """
     from qpop_diffraction_b200 import Plan, crystal_from, replicas, workloads
-    shape = tuple(args.grid) if tuple(args.grid) != GRID else CONFIG3
     params, inputs = workloads.gpu_snapshot("twin", shape, seed=3 + rank, device=dev, n_phase=1)
-    crystal = crystal_from(params, workloads.config3_crystal(3, (1, 1, 3)))
+    atoms = workloads.config3_crystal(3, (1, 1, 3))
+    crystal = crystal_from(params, atoms)
+    spacing = (params.dx, params.dy, params.dz)
     n = params.n
     torch.cuda.synchronize(dev)
     torch.cuda.empty_cache()
-    plan = Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp32", device=dev.index)
+    torch.cuda.reset_peak_memory_stats(dev)
+    plan = Plan(shape, spacing, 1, 3, precision="fp32", device=dev.index)
     plan.set_crystal(crystal)
     out = torch.empty(shape, dtype=torch.float64, device=dev)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         plan.run_device(inputs, out)
     torch.cuda.synchronize(dev)
     plan.device_status()
@@ -230,56 +288,119 @@ def run_config3(args, torch, dev, rank, world):
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         plan.run_device(inputs, out)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     plan.device_status()
-    ms = replicas.slowest(e0.elapsed_time(e1), dev) / args.steps
+    ms = replicas.slowest(e0.elapsed_time(e1), dev) / steps
     stage = plan.stage_times()
+    plan.enable_timing(False)
     hbm, hbm_src = peaks()
     g1, g2 = atom_groups(crystal.R)
     kb = kernel_bytes(n, g1, g2, False)
     kernels = {k: {"avg_ms": t / c, "bytes_per_launch": kb[k], "gbs": kb[k] / (t / c * 1e-3) / 1e9,
                    "frac": kb[k] / (t / c * 1e-3) / 1e9 / hbm} for k, (t, c) in stage.items() if k in kb}
-    line = {"metric": f"Gcells/s per 3-D volume at {'x'.join(map(str, shape))} (float32, one GPU)",
-            "value": replicas.throughput(n, ms * 1e-3, world) / 1e9, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "dtype": "f32", "data": "synthetic (seeded Voronoi twin film, generated on the GPU)",
-            "config": {"workload": f"three-variant Voronoi twin film {'x'.join(map(str, shape))}, 200 domains, "
-                                   f"5 atoms, 1 phase, G=113", "cells": n},
-            "kernels": kernels, "peak_gbs": hbm, "peak_source": f"hbm_gbs of {hbm_src}",
-            "device_memory_peak_gb": (torch.cuda.max_memory_allocated(dev) + plan.workspace_bytes) / 1e9}
-    if args.validate:
-        I32 = out
+    res = {"workload": f"three-variant Voronoi twin film {'x'.join(map(str, shape))}, 200 domains, 5 atoms, "
+                       f"1 phase, G=113, generated on the GPU", "cells": n, "steps": steps, "warmup": warmup,
+           "ms_per_volume": ms, "value": replicas.throughput(n, ms * 1e-3, world) / 1e9, "unit": UNIT,
+           "kernels": kernels, "peak_gbs": hbm, "peak_source": f"hbm_gbs of {hbm_src}",
+           "device_memory_peak_gb": (torch.cuda.max_memory_allocated(dev) + plan.workspace_bytes) / 1e9}
+    if direct:
+        sys.path.insert(0, str(ROOT / "tests"))
+        from direct_dft import crystal_constants, direct_intensity, fft_index_to_shifted, shifted_to_fft_index
+        top = torch.topk(out.view(-1), 32).indices.cpu().numpy()
+        sx, sy, sz = np.unravel_index(top, shape)
+        inv = [shifted_to_fft_index(m) for m in shape]
+        bright = np.stack([inv[0][sx], inv[1][sy], inv[2][sz]], axis=1)
+        rng = np.random.default_rng(11)
+        vox = np.concatenate([bright, np.stack([rng.integers(0, m, 32) for m in shape], axis=1)])
+        pos = [fft_index_to_shifted(m) for m in shape]
+        sel = [torch.from_numpy(pos[d][vox[:, d]]).to(dev) for d in range(3)]
+        got = out[sel[0], sel[1], sel[2]].cpu().numpy()
         plan.close()
-        del plan
+        del out
         torch.cuda.empty_cache()
-        in64 = {"P": inputs["P"].double(), "U": inputs["U"].double(), "phase": inputs["phase"], "weight": None,
-                "wdense": None}
-        del inputs
-        torch.cuda.empty_cache()
-        p64 = Plan(shape, (params.dx, params.dy, params.dz), 1, 3, precision="fp64", schedule="plain",
-                   device=dev.index)
-        p64.set_crystal(crystal)
-        I64 = torch.empty(shape, dtype=torch.float64, device=dev)
         t = time.perf_counter()
-        p64.run_device(in64, I64)
-        torch.cuda.synchronize(dev)
-        p64.device_status()
-        t64 = time.perf_counter() - t
-        imax = I64.max()
-        strong = I64 > 1e-6 * imax
-        line["validation"] = {
-            "against": "float64 plain schedule of the same kernels on the full grid",
-            "max_abs_dI_over_Imax": float((I32 - I64).abs().max() / imax),
-            "max_rel_err_above_1e-6_Imax": float(((I32 - I64).abs()[strong] / I64[strong]).max()),
-            "max_abs_dlog10I_above_1e-6_Imax": float((torch.log10(I32[strong]) - torch.log10(I64[strong])).abs().max()),
-            "fp64_plain_seconds": t64}
-        p64.close()
+        want = direct_intensity(torch, shape, spacing, *crystal_constants(params, atoms), inputs["P"], inputs["U"],
+                                inputs["phase"], inputs["weight"], vox)
+        imax = want.max()
+        big = want > 1e-6 * imax
+        res["direct_sums"] = {"voxels": int(len(vox)), "voxels_above_1e-6_Imax": int(big.sum()),
+                              "max_abs_dI_over_Imax": float(np.abs(got - want).max() / imax),
+                              "max_rel_err_above_1e-6_Imax": float((np.abs(got - want)[big] / want[big]).max()),
+                              "seconds": time.perf_counter() - t,
+                              "against": "float64 direct sums over all cells (no FFT), 32 brightest + 32 random voxels"}
     else:
         plan.close()
+        del out
+    if validate:
+        torch.cuda.empty_cache()
+        out32 = None
+        p32 = Plan(shape, spacing, 1, 3, precision="fp32", device=dev.index)
+        p32.set_crystal(crystal)
+        out32 = p32.run_device(inputs).cpu()
+        p32.close()
+        in64 = {"P": inputs["P"].double(), "U": inputs["U"].double(), "phase": inputs["phase"], "weight": None,
+                "wdense": None}
+        torch.cuda.empty_cache()
+        p64 = Plan(shape, spacing, 1, 3, precision="fp64", schedule="plain", device=dev.index)
+        p64.set_crystal(crystal)
+        t = time.perf_counter()
+        I64 = p64.run_device(in64)
+        torch.cuda.synchronize(dev)
+        p64.device_status()
+        res["validation"] = dict(intensity_errors(out32.numpy(), I64.cpu().numpy()),
+                                 against="float64 plain schedule of the same kernels on the full grid",
+                                 fp64_plain_seconds=time.perf_counter() - t)
+        p64.close()
+        del in64, I64
+        torch.cuda.empty_cache()
+    if e2e:
+        import psutil
+        if psutil.virtual_memory().available < 120e9:
+            res["e2e"] = {"skipped": "needs about 90 GB of free host memory for the float64 host arrays"}
+        else:
+            # the reference layout on the host: float64 oPhase, oStruc (P), u, region, as cli.py hands them over
+            host = {"oStruc": inputs["P"].reshape(-1).cpu().numpy().astype(np.float64),
+                    "u": inputs["U"].reshape(-1).cpu().numpy().astype(np.float64)}
+            ph = inputs["phase"].reshape(-1).cpu().numpy()
+            host["oPhase"] = (ph == 0).astype(np.float64)
+            host["region"] = (ph >= 0).astype(np.float64)
+            del ph, inputs
+            torch.cuda.empty_cache()
+            I_host = np.empty(shape, dtype=np.float64)
+            ph = Plan(shape, spacing, 1, 3, precision="fp32", device=dev.index)
+            ph.set_crystal(crystal)
+            ph.run_host(host["oPhase"], host["oStruc"], host["u"], host["region"], out=I_host)  # workspace, ring
+            ph.stage_times()
+            ph.enable_timing(True)
+            t = time.perf_counter()
+            ph.run_host(host["oPhase"], host["oStruc"], host["u"], host["region"], out=I_host)
+            total = time.perf_counter() - t
+            kern = sum(v[0] for v in ph.stage_times().values())
+            h2d = sum(a.nbytes for a in host.values())
+            res["e2e"] = {"value": n / total / 1e9, "unit": UNIT, "seconds": total, "kernels_ms": kern,
+                          "host_transfer_and_pack_ms": total * 1e3 - kern, "h2d_bytes": h2d, "d2h_bytes": I_host.nbytes,
+                          "call": "qpd_run_host: float64 host arrays in the reference layout (pageable), the intensity "
+                                  "back in a float64 host array"}
+            ph.close()
+            del host, I_host
+    return res
+
+
+def run_config3(args, torch, dev, rank, world):
+    """bench.py --config 3: the config-3 leg alone, one JSON line (--validate adds the float64 run)."""
+    shape = tuple(args.grid) if tuple(args.grid) != GRID else CONFIG3
+    res = config3_leg(args, torch, dev, rank, world, shape=shape, steps=args.steps, warmup=args.warmup,
+                      validate=args.validate, direct=shape == CONFIG3, e2e=shape == CONFIG3 and args.e2e_steps != 0)
     if rank == 0:
+        line = {"metric": f"Gcells/s per 3-D volume at {'x'.join(map(str, shape))} (float32, one GPU)",
+                "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": res["ms_per_volume"], "higher_is_better": True, "scaling": "weak", "dtype": "f32",
+                "data": "synthetic (seeded Voronoi twin film, generated on the GPU)",
+                "config": {"workload": res["workload"], "cells": res["cells"]}}
+        line.update({k: v for k, v in res.items() if k not in ("value", "workload", "cells")})
         print(json.dumps(line), flush=True)
 
 
@@ -309,14 +430,22 @@ def serving_leg(args, torch, device):
             eng.reserve(i, 2)
         eng.warm([(i, h) for i in range(32) for h in SERVING_HKLS])
         ids = list(range(32))
+        shape_of = lambda r: "x".join(map(str, store[r.snapshot].shape))
         cap = latency_stats(eng.run(poisson_requests(args.serving_requests, 0, ids, SERVING_HKLS, seed=1)))
-        rate = 0.8 * cap["volumes_per_s"]
-        load = latency_stats(eng.run(poisson_requests(args.serving_requests, rate, ids, SERVING_HKLS, seed=2)))
+        loads = {}
+        for i, frac in enumerate((0.5, 0.8, 0.95)):
+            rate = frac * cap["volumes_per_s"]
+            st = latency_stats(eng.run(poisson_requests(args.serving_requests, rate, ids, SERVING_HKLS, seed=2 + i)),
+                               key=shape_of)
+            loads[f"{int(frac * 100)}%"] = dict(st, offered_rate_per_s=rate)
+        load = loads["80%"]
         out = {"grids": [list(s) for s in SERVING_SHAPES], "snapshots": 32, "reflections": [list(h) for h in SERVING_HKLS],
-               "capacity_volumes_per_s": cap["volumes_per_s"], "offered_rate_per_s": rate, "p50_ms": load["p50_ms"],
-               "p99_ms": load["p99_ms"], "volumes_per_s": load["volumes_per_s"], "requests": load["requests"],
+               "capacity_volumes_per_s": cap["volumes_per_s"], "offered_rate_per_s": load["offered_rate_per_s"],
+               "p50_ms": load["p50_ms"], "p99_ms": load["p99_ms"], "volumes_per_s": load["volumes_per_s"],
+               "requests": load["requests"], "loads": loads,
                "slots": eng.peak_slots, "hbm_budget_gb": budget / 1e9, "resident_snapshots_gb": store.nbytes / 1e9,
-               "latency": "arrival to completion on the device, open-loop Poisson arrivals at 80% of capacity"}
+               "latency": "arrival to completion on the device, open-loop Poisson arrivals; p50/p99 at 80% of capacity, "
+                          "loads: at 50, 80 and 95%, overall and per grid"}
     finally:
         eng.close()
     return out
@@ -468,6 +597,7 @@ def main():
     ms = replicas.slowest(ms, dev)
     value = replicas.throughput(args.steps * n, ms * 1e-3, world) / 1e9
     I32 = plans[0].run_device(packed).clone()      # G = 002, for the float32-vs-float64 accuracy
+    I32_host = I32.cpu().numpy()
 
     hbm, hbm_src = peaks()
     weight = packed["weight"] is not None
@@ -481,7 +611,9 @@ def main():
     traffic = profiled_traffic()
     roof = {"bound": "hbm", "kernel": dom, "achieved": per_kernel[dom]["gbs"], "peak": hbm, "unit": "GB/s",
             "frac": per_kernel[dom]["gbs"] / hbm, "peak_source": f"hbm_gbs of {hbm_src}",
-            "traffic": traffic[dom] * n if dom in traffic else None}
+            "traffic": traffic[dom] * n if dom in traffic else None,
+            "traffic_source": "committed constant: ncu dram__bytes_read.sum + dram__bytes_write.sum per cell of this "
+                              "kernel in profiles/ (a smaller capture of the same kernel), times the cells of one launch"}
     model_bytes = n * 5 * (25 + 144)
     model = {"bytes_per_cell": 5 * (25 + 144), "achieved_gbs": model_bytes / (ms / args.steps * 1e-3) / 1e9,
              "frac": model_bytes / (ms / args.steps * 1e-3) / 1e9 / hbm}
@@ -532,16 +664,10 @@ def main():
             fp64[schedule] = {"value": n / (t * 1e-3) / 1e9, "ms_per_step": t, "steps": k}
             if schedule == "plain":
                 I64 = ps[0].run_device(pk)
-                imax = I64.max()
-                strong = I64 > 1e-6 * imax
-                dlog = (torch.log10(I32) - torch.log10(I64)).abs()
-                accuracy = {"against": "float64 plain schedule (the reference's per-atom loop), G=002, full grid",
-                            "max_abs_over_Imax": ((I32 - I64).abs().max() / imax).item(),
-                            "max_rel_above_1e-6_Imax": ((I32 - I64).abs()[strong] / I64[strong]).max().item(),
-                            "log10_I_max_err_above_1e-6_Imax": dlog[strong].max().item(),
-                            "log10_I_p99_err_all": torch.quantile(dlog.flatten()[::97].float(), 0.99).item(),
-                            "contract": "max |dI|/I_max <= 1e-5, rel <= 1e-3 above 1e-6 I_max"}
-                del I64, strong, dlog
+                accuracy = {"vs_fp64_plain": dict(intensity_errors(I32_host, I64.cpu().numpy()),
+                                                  against="float64 plain schedule of the same kernels (the "
+                                                          "reference's per-atom loop), G=002, full grid")}
+                del I64
             for p in ps:
                 p.close()
             del pk
@@ -562,16 +688,36 @@ def main():
         torch.cuda.empty_cache()
         serving = serving_leg(args, torch, local)
 
-    # ---------------- CPU baseline ----------------
+    # ---------------- 4000 x 4000 x 68 on one GPU ----------------
+    config3 = None
+    if world == 1 and not args.no_config3:
+        torch.cuda.empty_cache()
+        config3 = config3_leg(args, torch, dev, rank, world, e2e=False)  # e2e from host arrays: bench.py --config 3
+
+    # ---------------- CPU baseline: the reference itself on the full grid ----------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        from oracle import diffraction_oracle as oracle
-        threads = oracle.default_threads(5)
-        rate, dt = cpu_oracle_rate(CPU_SAMPLE, threads)
-        cpu = {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"oracle (NumPy restatement of the reference diffraction()) on the config-2 snapshot cropped "
-                         f"to {'x'.join(map(str, CPU_SAMPLE))}, G=002, one run of {dt:.1f} s, "
-                         f"{threads} atom threads on {os.cpu_count()} host cores"}
+        from qpop_diffraction_b200.diffraction import q_axes
+        diffraction = reference_diffraction()
+        kind = "reference"
+        if diffraction is None:  # no install and no checkout: the oracle port, the same algorithm restated
+            from oracle import diffraction_oracle as oracle
+            diffraction, kind = oracle.diffraction, "port"
+        atoms = workloads.config2_crystal(2, REFLECTIONS[0])
+        t = time.perf_counter()
+        Iref, qx, qy, qz = diffraction(params, atoms, oPhase, oStruc, u, region)
+        dt = time.perf_counter() - t
+        who = ("the reference's own diffraction() (baseline/_ref, unmodified, NumPy as installed)" if kind == "reference"
+               else "the oracle port of the reference's diffraction() (NumPy)")
+        cpu = {"value": n / dt / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+               "sample": f"{who} on the full {'x'.join(map(str, shape))} config-2 grid, G=002, one run of "
+                         f"{dt:.1f} s; host {host_cpu()}"}
+        ours = q_axes(params, crystals[0].qC)
+        accuracy = accuracy or {}
+        accuracy["vs_reference"] = dict(intensity_errors(I32_host, Iref),
+                                        against=f"{who}, G=002, full grid (float64)",
+                                        q_axes_bit_exact=all(np.array_equal(a, b) for a, b in zip(ours, (qx, qy, qz))))
+        del Iref
 
     if rank == 0:
         line = {
@@ -584,7 +730,8 @@ def main():
                        "l2": "no flush: every step reads and writes about 4 GB, far above the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "roofline": roof, "model_roofline": model, "kernels": per_kernel, "gpu_launches": launches,
-            "e2e": e2e, "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "serving": serving, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "e2e": e2e, "fp64": fp64, "accuracy": accuracy, "adjoint": adjoint, "serving": serving, "config3": config3,
+            "cpu_baseline": cpu, "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

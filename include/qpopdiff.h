@@ -161,6 +161,15 @@ QPD_API int qpd_adjoint_device(qpd_ctx* ctx, const void* P, const void* U, const
  * qpd_run_host checks this itself; callers of qpd_run_device call it after synchronising. */
 QPD_API int qpd_device_status(qpd_ctx* ctx);
 
+/* No counterpart in the reference (its failures abort through MPI_Abort, src/heffte/util.hpp:12-16).
+ * Runs the bounded-wait failure path once, on the context's stream, and waits for it: a kernel arms a
+ * shared-memory barrier for bytes that no copy ever delivers and gives up after `polls` polls
+ * (1 <= polls <= 2^24), recording a timeout in the context's device status word exactly as a
+ * TMA-fed kernel does when a tile load never lands.  qpd_device_status then returns QPD_ERR_CUDA and
+ * clears the word.  For tests of the error path: nothing is loaded, nothing faults and the context
+ * stays usable. */
+QPD_API int qpd_probe_wait_timeout(qpd_ctx* ctx, int64_t polls);
+
 /* Device bytes the context holds, and kernels it has launched since creation. */
 QPD_API uint64_t qpd_workspace_bytes(const qpd_ctx* ctx);
 QPD_API uint64_t qpd_launch_count(const qpd_ctx* ctx);

@@ -25,7 +25,7 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libqpopdiff.so"
 OBJ = PKG / "_build"
 
-SOURCES = ["qpd_api.cu", "qpd_noalloc.cu", "qpd_rsm.cu", "qpd_n4000.cu"]
+SOURCES = ["qpd_api.cu", "qpd_noalloc.cu", "qpd_rsm.cu", "qpd_n4000.cu", "qpd_probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

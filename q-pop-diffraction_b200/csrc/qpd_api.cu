@@ -24,6 +24,11 @@
 #include "qpd_kernels.cuh"
 #include "qpd_n4000.h"
 
+namespace qpd {
+// qpd_probe.cu: a kernel that takes the bounded-wait failure path (a barrier no copy completes)
+cudaError_t launch_wait_probe(int* status, long long polls, cudaStream_t st);
+}  // namespace qpd
+
 using namespace qpd;
 
 namespace {
@@ -1040,6 +1045,13 @@ template <typename T> struct Impl {
             case 1024: return fast_axis_n<1024, 1024, EPI, Radix<8, 8, 4, 4>>(c, a, nouter, kind, st);
             case 4000:
                 if constexpr (sizeof(T) == 4) {
+                    if (c->knob_n4k && c->tma && kind == QPD_K_YPASS && c->have_p4y && a.nz == 1 && !a.accumulate) {
+                        // one z value: every y pencil is contiguous, so the bulk y pass reads it whole
+                        cudaEvent_t t0;
+                        QPD_TRY(tstart(c, st, &t0));
+                        QPD_CU(c, launch_ypass4000(a, c->p4y, c->nx, st));
+                        return tstop(c, kind, st, t0);
+                    }
                     const bool yp = kind == QPD_K_YPASS && c->have_p4y, xp4 = kind == QPD_K_XPASS && c->have_p4x;
                     if (c->knob_n4k && c->tma && a.nz % 2 == 0 && !a.accumulate && (yp || xp4)) {
                         // register-resident passes over tiles of two neighbouring z values: rows along y for the y
@@ -1982,6 +1994,15 @@ int qpd_device_status(qpd_ctx* c) {
     if (!c) return fail(c, QPD_ERR_ARG, "qpd_device_status: ctx is NULL");
     QPD_TRY(use_device(c));
     return check_status(c);
+}
+
+int qpd_probe_wait_timeout(qpd_ctx* c, int64_t polls) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_probe_wait_timeout: ctx is NULL");
+    if (polls < 1 || polls > kWaitLimit) return fail(c, QPD_ERR_ARG, "polls outside 1..2^24");
+    QPD_TRY(use_device(c));
+    QPD_CU(c, launch_wait_probe(static_cast<int*>(c->status.p), (long long)polls, c->stream));
+    QPD_CU(c, cudaStreamSynchronize(c->stream));
+    return QPD_OK;
 }
 
 uint64_t qpd_workspace_bytes(const qpd_ctx* c) { return c ? c->held : 0; }

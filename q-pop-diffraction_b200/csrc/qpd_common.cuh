@@ -19,6 +19,10 @@ template <typename C> __host__ __device__ __forceinline__ C cmake(decltype(C::x)
     c.y = im;
     return c;
 }
+// The intensity floor max(v, 1e-50) as numpy.maximum computes it (src/python/diffraction.py:111): a NaN
+// propagates, where fmax would return the floor.
+__device__ __forceinline__ double floor_1e50(double v) { return v < 1e-50 ? 1e-50 : v; }
+
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return cmake<C>(a.x + b.x, a.y + b.y); }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { return cmake<C>(a.x - b.x, a.y - b.y); }
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {

@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(NT) axis_fast(AxisArgs<T> a) {
                         if (c + w < cz) {
                             const double S = sxy * a.S[2][kz];
                             const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
-                            const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
+                            const double v = floor_1e50(S * S * (re * re + im * im) * a.scale2);
                             a.I[row + fftshift_at(kz, a.nz)] = v;
                         }
                     }
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                         if (c + w < cz) {
                             const double S = sxz * a.S[1][ky];
                             const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
-                            const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
+                            const double v = floor_1e50(S * S * (re * re + im * im) * a.scale2);
                             a.I[(row + fftshift_at(ky, (int)a.ny)) * nzr + sz] = v;
                         }
                     }
@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(NT, NT <= 512 && sizeof(C_t<T>) * (N * CZ * (N
                         if (c + w < cz) {
                             const double S = sxy * a.S[2][kz];
                             const double re = (double)acc[0][q][w].x, im = (double)acc[0][q][w].y;
-                            const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
+                            const double v = floor_1e50(S * S * (re * re + im * im) * a.scale2);
                             a.I[row + fftshift_at(kz, a.nz)] = v;
                         }
                     }

@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(NT) axis_kernel(AxisArgs<T> a) {
                     const double S = a.S[0][kx] * syv * a.S[2][kz];
                     const double re = (double)acc[0][q].x, im = (double)acc[0][q].y;
                     double v = S * S * (re * re + im * im) * a.scale2;
-                    v = fmax(v, 1e-50);
+                    v = floor_1e50(v);
                     const long long sx = (kx + a.nx / 2) % a.nx;
                     const long long sz = (kz + a.nz / 2) % a.nz;
                     a.I[(sx * a.ny + sy) * a.nz + sz] = v;
@@ -742,7 +742,7 @@ template <typename T> __global__ void intensity_kernel(IntensityArgs<T> a) {
     const long long x = g / (a.nz * a.ny);
     const double S = a.S[0][x] * a.S[1][y] * a.S[2][z];
     const double re = (double)a.amp[g].x, im = (double)a.amp[g].y;
-    const double v = fmax(S * S * (re * re + im * im) * a.scale2, 1e-50);
+    const double v = floor_1e50(S * S * (re * re + im * im) * a.scale2);
     const long long sx = (x + a.nx / 2) % a.nx, sy = (y + a.ny / 2) % a.ny, sz = (z + a.nz / 2) % a.nz;
     a.I[(sx * a.ny + sy) * a.nz + sz] = v;
 }

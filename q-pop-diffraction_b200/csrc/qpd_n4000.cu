@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
                         const int kx = tt + 200 * r;
                         const double Sx = a.S[0][kx] * syz;
                         const double re = (double)acc[r].x, im = (double)acc[r].y;
-                        const double val = fmax(Sx * Sx * (re * re + im * im) * a.scale2, 1e-50);
+                        const double val = floor_1e50(Sx * Sx * (re * re + im * im) * a.scale2);
                         a.I[((long long)shift_at(kx, nfx) * NY + sy) * NZ + sz] = val;
                     }
                 } else {

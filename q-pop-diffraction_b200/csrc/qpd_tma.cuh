@@ -56,9 +56,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of bar; false (and the status word set) when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
-    for (long long it = 0; it < kWaitLimit; it++)
+// Bounded wait for phase `parity` of bar, at most `limit` polls; false (and the status word set) when it
+// gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, long long limit = kWaitLimit) {
+    for (long long it = 0; it < limit; it++)
         if (mbar_try_wait(bar, parity)) return true;
     if (status) atomicExch(status, QPD_DEVERR_TIMEOUT);
     return false;

@@ -129,6 +129,10 @@ class Plan:
         """Raise if a kernel of this plan gave up on a bounded wait (reads and clears the device status)."""
         self._check(self.lib.qpd_device_status(self._ctx))
 
+    def probe_wait_timeout(self, polls=1000):
+        """Run the bounded-wait failure path once (qpd_probe_wait_timeout); device_status() then raises."""
+        self._check(self.lib.qpd_probe_wait_timeout(self._ctx, int(polls)))
+
     def enable_timing(self, on=True):
         """Record CUDA events around every kernel launch (see stage_times)."""
         self._check(self.lib.qpd_enable_timing(self._ctx, int(bool(on))))

@@ -72,6 +72,7 @@ class Request:
     start: float = None       # dispatch time
     done: float = None        # completion seen by the host
     slot: object = None
+    cancelled: bool = False   # cancelled before it ran (start None) or while it ran (its result discarded)
 
     @property
     def latency(self):
@@ -181,6 +182,19 @@ class Engine:
     def busy(self):
         return any(s.request is not None for v in self.slots.values() for s in v)
 
+    def release_idle(self):
+        """Close every slot without a request in flight and return its footprint to the budget."""
+        for shape in list(self.slots):
+            keep = []
+            for s in self.slots[shape]:
+                if s.request is None:
+                    self.used -= s.footprint
+                    s.close()
+                else:
+                    keep.append(s)
+            self.slots[shape] = keep
+        return self.used
+
     def reserve(self, snap_id, count):
         """Create up to `count` slots for a snapshot's shape, as far as the budget allows."""
         snap = self.store[snap_id]
@@ -196,13 +210,19 @@ class Engine:
                 s.launch(snap, hkl)
                 s.stream.synchronize()
 
-    def run(self, requests, result_of=None):
+    def run(self, requests, result_of=None, cancel=()):
         """
         Serve requests (arrival times in seconds from now, sorted).  Returns them with start and done
         times set.  result_of(request, tensor) is called on completion with the slot's output.
+
+        cancel: (time, request id) pairs.  At that time a request still queued is dropped (returned with
+        cancelled set and start None); one already on the device finishes there (a graph in flight is
+        not interrupted), its result is discarded and its slot is free for the next request.
         """
         waiting = collections.deque()
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        cancels = collections.deque(sorted(cancel))
+        by_id = {r.id: r for r in requests}
         finished = []
         t0 = time.perf_counter()
         while pending or waiting or self.busy():
@@ -214,10 +234,24 @@ class Engine:
                 r = waiting.popleft()
                 if not self.dispatch(r, time.perf_counter() - t0):
                     waiting.append(r)
+            # cancellations due by now, after this round's dispatch
+            while cancels and cancels[0][0] <= now:
+                r = by_id.get(cancels.popleft()[1])
+                if r is None or r.done is not None or r.cancelled:
+                    continue
+                r.cancelled = True
+                if r.start is None:  # still queued: it never reaches the device
+                    if r in pending:
+                        pending.remove(r)
+                    if r in waiting:
+                        waiting.remove(r)
+                    finished.append(r)
             done_before = len(finished)
             self.poll(time.perf_counter() - t0, finished)
             if result_of is not None:
                 for r in finished[done_before:]:
+                    if r.cancelled:
+                        continue
                     r.slot.stream.synchronize()
                     result_of(r, r.slot.out)
             if not (waiting or pending) and not self.busy():
@@ -242,8 +276,20 @@ def poisson_requests(n, rate, snapshots, hkls, seed=0):
     return [Request(i, int(snapshots[snaps[i]]), tuple(hkls[hk[i]]), float(t[i])) for i in range(n)]
 
 
-def latency_stats(finished):
+def latency_stats(finished, key=None):
+    """
+    p50 / p99 / mean latency and volumes per second of the requests that completed (cancelled ones are
+    left out); with key(request) also the same figures per key (for example the grid shape).
+    """
+    finished = [r for r in finished if not r.cancelled]
     lat = np.array([r.latency for r in finished])
     span = max(r.done for r in finished) - min(r.arrival for r in finished)
-    return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-            "mean_ms": float(lat.mean() * 1e3), "volumes_per_s": len(finished) / span, "requests": len(finished)}
+    out = {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+           "mean_ms": float(lat.mean() * 1e3), "volumes_per_s": len(finished) / span, "requests": len(finished)}
+    if key is not None:
+        groups = collections.defaultdict(list)
+        for r in finished:
+            groups[key(r)].append(r.latency)
+        out["by"] = {str(k): {"p50_ms": float(np.percentile(v, 50) * 1e3), "p99_ms": float(np.percentile(v, 99) * 1e3),
+                              "requests": len(v)} for k, v in sorted(groups.items())}
+    return out

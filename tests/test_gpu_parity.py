@@ -94,7 +94,7 @@ def test_edge_shapes(gpu, shape, precisions):
 
 @pytest.mark.parametrize("shape", [(512, 2, 104), (2, 512, 104), (256, 128, 64), (128, 256, 68), (1024, 2, 32),
                                    (2, 1024, 128), (32, 64, 128), (64, 32, 32), (512, 2, 7), (2, 256, 9),
-                                   (4000, 2, 68), (2, 4000, 68)])
+                                   (4000, 2, 68), (2, 4000, 68), (3, 4000, 1)])
 def test_specialised_axis_lengths(gpu, shape):
     """Every axis length with a compile-time kernel, in both strided positions, even and odd nz."""
     from qpop_diffraction_b200 import workloads

@@ -94,3 +94,36 @@ def test_served_volume_meets_the_contract(gpu):
         ref = oracle.diffraction(snap.params, workloads.serving_crystal(HKLS[i % 4]), oPhase, P, U, region)[0]
         dmax, rel = fp32_errors(out[i], ref)
         assert dmax <= 1e-5 and rel <= 1e-3, (snap.shape, dmax, rel)
+
+
+def test_cancel_queued_and_in_flight_requests(gpu):
+    """A queued request cancelled never runs; one cancelled on the device finishes there with its
+    result discarded; the slot serves the next request, which gives the same volume as when run alone;
+    releasing idle slots returns their footprint to the budget."""
+    torch = gpu
+    from qpop_diffraction_b200.serving import Engine, Request
+    store = make_store(torch, n_per_shape=1)
+    shape_snap = 2  # (48, 32, 104)
+    eng = Engine(store, hbm_budget_bytes=4 << 30)
+    try:
+        assert eng.reserve(shape_snap, 1) == 1
+        budget_used = eng.budget = eng.used  # no room for a second slot: the shape has exactly one
+        alone = {}
+        eng.run([Request(9, shape_snap, (1, 0, 3), 0.0)], result_of=lambda q, t: alone.__setitem__(q.id, t.cpu().numpy()))
+        assert len(eng.slots[store[shape_snap].shape]) == 1
+        reqs = [Request(0, shape_snap, (0, 0, 2), 0.0), Request(1, shape_snap, (2, 0, 0), 0.0),
+                Request(2, shape_snap, (1, 0, 3), 0.0)]
+        got = {}
+        out = eng.run(reqs, result_of=lambda q, t: got.__setitem__(q.id, t.cpu().numpy()),
+                      cancel=[(0.0, 1), (0.0, 0)])
+        by = {r.id: r for r in out}
+        assert sorted(by) == [0, 1, 2]
+        assert by[1].cancelled and by[1].start is None and by[1].done is None       # dropped from the queue
+        assert by[0].cancelled and by[0].start is not None and by[0].done is not None  # finished, discarded
+        assert not by[2].cancelled and by[2].done is not None
+        assert sorted(got) == [2]
+        np.testing.assert_array_equal(got[2], alone[9])
+        assert not eng.busy() and eng.used == budget_used
+        assert eng.release_idle() == 0
+    finally:
+        eng.close()
