@@ -408,7 +408,13 @@ SERVING_SHAPES = ((128, 128, 128), (256, 256, 64), (512, 512, 104), (1024, 1024,
 SERVING_HKLS = ((0, 0, 2), (1, 0, 3), (1, 1, 3), (2, 0, 0))
 
 
-def serving_leg(args, torch, device):
+# Engine options of the serving leg: stream priorities by grid size and at most two volumes in flight per
+# grid (measured on one B200: capacity 306 against 219 volumes/s with unlimited slots and no priorities,
+# p50 at 80% load 3.8 against 9.9 ms)
+SERVING_POLICY = {"priorities": True, "max_slots": 2}
+
+
+def serving_leg(args, torch, device, policy=None):
     """
     32 resident snapshots (8 per grid of the serving mix, vortex / twin / two-phase textures) and
     Poisson requests over them and the 4 reflections.  Capacity: every request queued at once; then
@@ -424,7 +430,8 @@ def serving_leg(args, torch, device):
         store.add(Snapshot(i, kind, shape, params, inputs))
     free, total = torch.cuda.mem_get_info(device)
     budget = int(min(free - (8 << 30), 64 << 30))
-    eng = Engine(store, budget, device=device)
+    policy = SERVING_POLICY if policy is None else policy
+    eng = Engine(store, budget, device=device, **policy)
     try:
         for i in range(4):                      # two slots per grid where the budget allows
             eng.reserve(i, 2)
@@ -443,7 +450,8 @@ def serving_leg(args, torch, device):
                "capacity_volumes_per_s": cap["volumes_per_s"], "offered_rate_per_s": load["offered_rate_per_s"],
                "p50_ms": load["p50_ms"], "p99_ms": load["p99_ms"], "volumes_per_s": load["volumes_per_s"],
                "requests": load["requests"], "loads": loads,
-               "slots": eng.peak_slots, "hbm_budget_gb": budget / 1e9, "resident_snapshots_gb": store.nbytes / 1e9,
+               "slots": eng.peak_slots, "policy": dict(policy), "hbm_budget_gb": budget / 1e9,
+               "resident_snapshots_gb": store.nbytes / 1e9,
                "latency": "arrival to completion on the device, open-loop Poisson arrivals; p50/p99 at 80% of capacity, "
                           "loads: at 50, 80 and 95%, overall and per grid"}
     finally:

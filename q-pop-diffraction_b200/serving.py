@@ -82,12 +82,12 @@ class Request:
 class Slot:
     """One in-flight volume's worth of resources for a grid shape."""
 
-    def __init__(self, shape, spacing, nPhase, device, crystal_of):
+    def __init__(self, shape, spacing, nPhase, device, crystal_of, priority=0):
         import torch
         self.shape, self.spacing = tuple(shape), tuple(spacing)
         self.plan = Plan(shape, spacing, nPhase, 3, precision="fp32", device=device)
         self.device = torch.device("cuda", device)
-        self.stream = torch.cuda.Stream(self.device)
+        self.stream = torch.cuda.Stream(self.device, priority=priority)
         self.out = torch.empty(self.shape, dtype=torch.float64, device=self.device)
         self.event = torch.cuda.Event()
         self.graphs = {}
@@ -125,11 +125,19 @@ class Slot:
 class Engine:
     """Admission by HBM footprint, per-shape slots, continuous dispatch."""
 
-    def __init__(self, store: SnapshotStore, hbm_budget_bytes, device=0, crystal_of=None):
+    def __init__(self, store: SnapshotStore, hbm_budget_bytes, device=0, crystal_of=None, priorities=False,
+                 max_slots=None):
+        """
+        priorities: give the slots of smaller grids higher CUDA stream priorities, so that when SMs free
+        up the block scheduler starts a small volume's kernels before a large one's.  max_slots: at most
+        this many slots (volumes in flight) per grid shape; None: as many as the budget holds.
+        """
         from . import workloads
         self.store = store
         self.budget = int(hbm_budget_bytes)
         self.device = device
+        self.priorities = priorities
+        self.max_slots = max_slots
         self.crystal_of = crystal_of or (lambda params, hkl: crystal_from(params, workloads.serving_crystal(hkl)))
         self.slots = collections.defaultdict(list)   # shape -> [Slot]
         self.used = 0
@@ -147,12 +155,26 @@ class Engine:
         probe_bytes = self._footprint_estimate(snap)
         if self.used + probe_bytes > self.budget:
             return None
+        if self.max_slots is not None and len(self.slots[snap.shape]) >= self.max_slots:
+            return None
         s = Slot(snap.shape, (params.dx, params.dy, params.dz), params.nPhase, self.device,
-                 lambda hkl, p=params: self.crystal_of(p, hkl))
+                 lambda hkl, p=params: self.crystal_of(p, hkl), priority=self._priority(snap.shape))
         self.used += s.footprint
         self.slots[snap.shape].append(s)
         self.peak_slots = max(self.peak_slots, sum(len(v) for v in self.slots.values()))
         return s
+
+    def _priority(self, shape):
+        """Stream priority of a grid's slots: the smallest grids highest (the lowest number)."""
+        if not self.priorities:
+            return 0
+        import torch
+        lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
+        sizes = sorted({int(np.prod(s.shape)) for s in self.store.snaps.values()})
+        rank = sizes.index(int(np.prod(shape))) if int(np.prod(shape)) in sizes else len(sizes) - 1
+        # hi is the greatest priority (most negative); spread the grids over the range, smallest first
+        levels = lo - hi
+        return hi + min(levels, round(rank * levels / max(1, len(sizes) - 1)))
 
     @staticmethod
     def _footprint_estimate(snap):
