@@ -24,6 +24,9 @@ Printed (rank 0, one JSON line):
             the float64 oracle of the full-grid accuracy figures;
   fp64      the same hand-written kernels in float64, fused and plain (the reference's own
             per-atom, per-component schedule), for the float32-vs-float64 comparison;
+  accuracy  float32 against float64: the reference itself at G=002 on the full grid, the float64
+            oracle per workload (configs 1, 2 at G=103, serving grids, the config-5 forward, direct
+            sums at 1024 x 1024 x 68), and the same kernels in float64;
   config3   the 4000 x 4000 x 68 twin film on one GPU: per-pass times and roofline fractions,
             device memory and float64 direct sums at 64 voxels (bench.py --config 3 adds one
             end-to-end volume from float64 host arrays through qpd_run_host).
@@ -77,6 +80,8 @@ def parse():
                     help="3: the 4000x4000x68 twin film on one GPU (device-resident, per-pass roofline)")
     ap.add_argument("--validate", action="store_true", help="with --config 3: compare against a float64 plain run")
     ap.add_argument("--no-config3", action="store_true", help="skip the 4000x4000x68 leg of the default run")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the per-workload float32-vs-float64-oracle leg of the default run")
     return ap.parse_args()
 
 
@@ -257,6 +262,103 @@ def intensity_errors(I, ref):
             "contract": "max |dI|/I_max <= 1e-5, rel <= 1e-3 above 1e-6 I_max"}
 
 
+def pick_voxels(torch, out, nbright=32, nrandom=32, seed=11):
+    """FFT-order indices of the brightest and of random voxels of a shifted volume, and their values."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from direct_dft import fft_index_to_shifted, shifted_to_fft_index
+    shape = tuple(out.shape)
+    top = torch.topk(out.view(-1), nbright).indices.cpu().numpy()
+    sx, sy, sz = np.unravel_index(top, shape)
+    inv = [shifted_to_fft_index(m) for m in shape]
+    bright = np.stack([inv[0][sx], inv[1][sy], inv[2][sz]], axis=1)
+    rng = np.random.default_rng(seed)
+    vox = np.concatenate([bright, np.stack([rng.integers(0, m, nrandom) for m in shape], axis=1)])
+    pos = [fft_index_to_shifted(m) for m in shape]
+    sel = [torch.from_numpy(pos[d][vox[:, d]]).to(out.device) for d in range(3)]
+    return vox, out[sel[0], sel[1], sel[2]].cpu().numpy()
+
+
+def direct_errors(torch, params, atoms, inputs, vox, got):
+    """The values `got` at voxels `vox` against float64 direct sums over all cells (tests/direct_dft.py)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from direct_dft import crystal_constants, direct_intensity
+    shape = (params.nx, params.ny, params.nz)
+    t = time.perf_counter()
+    want = direct_intensity(torch, shape, (params.dx, params.dy, params.dz), *crystal_constants(params, atoms),
+                            inputs["P"], inputs["U"], inputs["phase"], inputs["weight"], vox)
+    imax = want.max()
+    big = want > 1e-6 * imax
+    return {"voxels": int(len(vox)), "voxels_above_1e-6_Imax": int(big.sum()),
+            "max_abs_dI_over_Imax": float(np.abs(got - want).max() / imax),
+            "max_rel_err_above_1e-6_Imax": float((np.abs(got - want)[big] / want[big]).max()),
+            "max_abs_dlog10I_above_1e-6_Imax": float(np.abs(np.log10(got[big]) - np.log10(want[big])).max()),
+            "seconds": time.perf_counter() - t,
+            "against": f"float64 direct sums over all cells (no FFT), {len(vox) // 2} brightest + "
+                       f"{len(vox) - len(vox) // 2} random voxels"}
+
+
+def oracle_arrays(params, inputs):
+    """Float64 host arrays (oPhase, oStruc, u, region) in the reference layout holding packed device inputs."""
+    ph = inputs["phase"].cpu().numpy().astype(np.int64)
+    oPhase = np.concatenate([(ph == p).astype(np.float64) for p in range(params.nPhase)])
+    region = np.ones(ph.size) if inputs["weight"] is None else inputs["weight"].double().cpu().numpy()
+    return oPhase, inputs["P"].double().cpu().numpy(), inputs["U"].double().cpu().numpy(), region
+
+
+def accuracy_leg(torch, dev, config2=None):
+    """
+    The float32 fused path against the float64 oracle (the reference's diffraction() restated in NumPy,
+    pinned to the reference's own outputs by the golden tests) on each workload's own inputs:
+    config 1 through the drop-in diffraction() call, the config-2 grid at G=103 (G=002 is compared
+    with the reference itself by the CPU baseline), two serving grids, the config-5 forward, and the
+    1024 x 1024 x 68 serving grid by float64 direct sums at 64 voxels.  config2: (params, host arrays,
+    float32 volume at G=103) of the bench's config-2 snapshot.
+    """
+    import qpop_diffraction_b200 as qpd
+    from oracle import diffraction_oracle as oracle
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    threads = oracle.default_threads(5)
+    out = {}
+
+    def entry(name, I32, params, atoms, arrays):
+        t = time.perf_counter()
+        ref = oracle.diffraction(params, atoms, *arrays, threads=threads)[0]
+        out[name] = dict(intensity_errors(I32, ref), oracle_seconds=time.perf_counter() - t)
+
+    case = workloads.config1()
+    I32 = qpd.diffraction(*case.args(), device=dev.index)[0]
+    entry("config 1: 64x64x32 perovskite stripes, G=002 (drop-in diffraction())", I32, case.params, case.atoms,
+          (case.oPhase, case.oStruc, case.u, case.region))
+    if config2 is not None:
+        params, arrays, I32 = config2
+        entry(f"config 2: {'x'.join(map(str, GRID))} polar-vortex film, G=103", I32, params,
+              workloads.config2_crystal(2, (1, 0, 3)), arrays)
+    for kind, shape, seed, hkl, label in (("vortex", (128, 128, 128), 1000, (0, 0, 2), "serving"),
+                                          ("twin", (256, 256, 64), 1005, (1, 1, 3), "serving"),
+                                          ("vortex", (256, 256, 64), 5, (1, 0, 3), "config 5 forward")):
+        params, inputs = workloads.gpu_snapshot(kind, shape, seed=seed, device=dev)
+        atoms = workloads.serving_crystal(hkl)
+        with Plan(shape, (params.dx, params.dy, params.dz), params.nPhase, 3, precision="fp32",
+                  device=dev.index) as plan:
+            plan.set_crystal(crystal_from(params, atoms))
+            I32 = plan.run_device(inputs).cpu().numpy()
+        entry(f"{label}: {'x'.join(map(str, shape))} {kind} (seed {seed}), G={''.join(map(str, hkl))}", I32, params,
+              atoms, oracle_arrays(params, inputs))
+        del inputs
+    shape, hkl = (1024, 1024, 68), (1, 0, 3)
+    params, inputs = workloads.gpu_snapshot("twophase", shape, seed=1002, device=dev)
+    atoms = workloads.serving_crystal(hkl)
+    with Plan(shape, (params.dx, params.dy, params.dz), params.nPhase, 3, precision="fp32", device=dev.index) as plan:
+        plan.set_crystal(crystal_from(params, atoms))
+        vox, got = pick_voxels(torch, plan.run_device(inputs))
+    out[f"serving: {'x'.join(map(str, shape))} twophase (seed 1002), G=103, direct sums"] = \
+        direct_errors(torch, params, atoms, inputs, vox, got)
+    del inputs
+    torch.cuda.empty_cache()
+    return {"threads": threads, "cases": out,
+            "against": "float64 oracle on the same inputs (full volume), or float64 direct sums where marked"}
+
+
 def config3_leg(args, torch, dev, rank, world, shape=CONFIG3, steps=3, warmup=1, validate=False, direct=True,
                 e2e=True):
     """
@@ -307,30 +409,11 @@ def config3_leg(args, torch, dev, rank, world, shape=CONFIG3, steps=3, warmup=1,
            "kernels": kernels, "peak_gbs": hbm, "peak_source": f"hbm_gbs of {hbm_src}",
            "device_memory_peak_gb": (torch.cuda.max_memory_allocated(dev) + plan.workspace_bytes) / 1e9}
     if direct:
-        sys.path.insert(0, str(ROOT / "tests"))
-        from direct_dft import crystal_constants, direct_intensity, fft_index_to_shifted, shifted_to_fft_index
-        top = torch.topk(out.view(-1), 32).indices.cpu().numpy()
-        sx, sy, sz = np.unravel_index(top, shape)
-        inv = [shifted_to_fft_index(m) for m in shape]
-        bright = np.stack([inv[0][sx], inv[1][sy], inv[2][sz]], axis=1)
-        rng = np.random.default_rng(11)
-        vox = np.concatenate([bright, np.stack([rng.integers(0, m, 32) for m in shape], axis=1)])
-        pos = [fft_index_to_shifted(m) for m in shape]
-        sel = [torch.from_numpy(pos[d][vox[:, d]]).to(dev) for d in range(3)]
-        got = out[sel[0], sel[1], sel[2]].cpu().numpy()
+        vox, got = pick_voxels(torch, out)
         plan.close()
         del out
         torch.cuda.empty_cache()
-        t = time.perf_counter()
-        want = direct_intensity(torch, shape, spacing, *crystal_constants(params, atoms), inputs["P"], inputs["U"],
-                                inputs["phase"], inputs["weight"], vox)
-        imax = want.max()
-        big = want > 1e-6 * imax
-        res["direct_sums"] = {"voxels": int(len(vox)), "voxels_above_1e-6_Imax": int(big.sum()),
-                              "max_abs_dI_over_Imax": float(np.abs(got - want).max() / imax),
-                              "max_rel_err_above_1e-6_Imax": float((np.abs(got - want)[big] / want[big]).max()),
-                              "seconds": time.perf_counter() - t,
-                              "against": "float64 direct sums over all cells (no FFT), 32 brightest + 32 random voxels"}
+        res["direct_sums"] = direct_errors(torch, params, atoms, inputs, vox, got)
     else:
         plan.close()
         del out
@@ -606,6 +689,7 @@ def main():
     value = replicas.throughput(args.steps * n, ms * 1e-3, world) / 1e9
     I32 = plans[0].run_device(packed).clone()      # G = 002, for the float32-vs-float64 accuracy
     I32_host = I32.cpu().numpy()
+    I32_103 = plans[1].run_device(packed).cpu().numpy()
 
     hbm, hbm_src = peaks()
     weight = packed["weight"] is not None
@@ -695,6 +779,13 @@ def main():
         del d64
         torch.cuda.empty_cache()
         serving = serving_leg(args, torch, local)
+
+    # ---------------- float32 against the float64 oracle, per workload ----------------
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        torch.cuda.empty_cache()
+        accuracy = accuracy or {}
+        accuracy["per_workload"] = accuracy_leg(torch, dev, (params, (oPhase, oStruc, u, region), I32_103))
+    del I32_103
 
     # ---------------- 4000 x 4000 x 68 on one GPU ----------------
     config3 = None
