@@ -295,14 +295,26 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
                     }
                 }
                 __syncthreads();
-                if (a.yfast) {
-                    // y fastest: column c = x ny + y goes to (x nz + k_z) ny + y (yfast 1: (x, k_z, y) layout) or
-                    // to (k_z nx + x) ny + y (yfast 2: (k_z, x, y) layout); neighbouring threads take
-                    // neighbouring columns of one k_z (runs of up to M values)
+                if (a.yfast == 2) {
+                    // (k_z, x, y) layout: column c = x ny + y of k_z sits at k_z ncols + c, and the tile's columns
+                    // are t M .. t M + M - 1, so neighbouring threads write neighbouring columns of one k_z
+                    C* o = a.out + 3LL * g * a.fstride + t * M;
+                    const int mcols = ncell / NZ;
+                    for (int e = tid; e < ncell; e += NT) {
+                        const int kz = mcols == M ? e / M : e / mcols;  // full tiles divide by a constant
+                        const int m = e - kz * mcols;
+                        const long long d = kz * a.ncols + m;
+                        const int s = m * PS + (kz % N1) * N2 + kz % N2;
+                        o[d] = cadd(buf[s], buf[3 * PLANE + s]);
+                        o[a.fstride + d] = buf[PLANE + s];
+                        o[2 * a.fstride + d] = buf[2 * PLANE + s];
+                    }
+                } else if (a.yfast) {
+                    // (x, k_z, y) layout: column c = x ny + y goes to (x nz + k_z) ny + y; neighbouring threads
+                    // take neighbouring columns of one k_z (runs of up to M values)
                     C* o = a.out + 3LL * g * a.fstride;
                     const int mcols = ncell / NZ;
                     const long long x0 = t * M / a.ny, y0 = t * M - x0 * a.ny;  // the tile's first column
-                    const long long nxz = a.ncols / a.ny;
                     for (int e = tid; e < ncell; e += NT) {
                         const int kz = mcols == M ? e / M : e / mcols;  // full tiles divide by a constant
                         const int m = e - kz * mcols;
@@ -311,7 +323,7 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
                             y -= a.ny;
                             x += 1;
                         }
-                        const long long d = (a.yfast == 2 ? kz * nxz + x : x * NZ + kz) * a.ny + y;
+                        const long long d = (x * NZ + kz) * a.ny + y;
                         const int s = m * PS + (kz % N1) * N2 + kz % N2;
                         o[d] = cadd(buf[s], buf[3 * PLANE + s]);
                         o[a.fstride + d] = buf[PLANE + s];
