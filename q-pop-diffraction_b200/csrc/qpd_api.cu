@@ -1302,9 +1302,21 @@ template <typename T> struct Impl {
                         CUtensorMap map;
                         QPD_TRY(field_map(c, &map, const_cast<C*>(x.in), false, c->ny, c->nx, 3 * c->ng1 * c->nz, 4, 200,
                                           1));
+                        // the intensity is staged as (k_z, k_y, k_x) rows in a field slot the x pass does not
+                        // read (the y pass leaves its outputs in the first 2 G2 slots of 3 G1), then moved to I
+                        auto read_by_x = [&](int f) {
+                            for (int i = 0; i < c->p4x.n; i++)
+                                if (c->p4x.field[i] == f) return true;
+                            return false;
+                        };
+                        int slot = 0;
+                        while (read_by_x(slot)) slot++;
+                        if (slot >= 3 * c->ng1) return fail(c, QPD_ERR_STATE, "no free field slot for the staged intensity");
+                        x.Istage = reinterpret_cast<double*>(F + (int64_t)slot * n);
                         cudaEvent_t t0;
                         QPD_TRY(tstart(c, st, &t0));
                         QPD_CU(c, launch_strided4000(map, x, c->p4x, (int)c->nz, Strided4k::XPassYFast, st));
+                        QPD_CU(c, launch_unstage_intensity(x.Istage, I, c->nx, c->ny, c->nz, st));
                         return tstop(c, QPD_K_XPASS, st, t0);
                     }
                     return tma_axis_b<4000, 2, 512, 2, true, true, Radix<8, 4, 5, 5, 5>, 2, true, true>(c, x, c->nz,

@@ -307,6 +307,8 @@ template <typename T> struct AxisArgs {
     int* status;        // device status word: bounded waits record timeouts here
     const double* gI;   // adjoint seed (EPI 2): dL/dI, fftshifted like I
     int nouter;         // y-fastest x pass: the k_z extent (CTAs take k_z fastest)
+    double* Istage;     // y-fastest 4000-point x pass: intensity rows (k_z, k_y, k_x), k_x fastest, unshifted;
+                        // a separate kernel moves them to I (null: the epilogue writes I directly)
 };
 
 // EPI 0: store the folded fields; 1: intensity epilogue; 2: adjoint seed, the conjugate gradient

@@ -301,8 +301,13 @@ __global__ void __launch_bounds__(kT, 2) ypass4000(AxisArgs<float> a, const __gr
 // ---------------------------------------------------------------------------------------
 // Strided pass: a tile is the two pencils of inner values 2 b and 2 b + 1 at one outer index o (the
 // value at transform index x of pencil (o, i) is element (o, i, x) of the map's view); it arrives as
-// 20 tensor boxes of 200 rows x 16 bytes in the staging buffer, S[2 x + c].  Thread 32 w + 16 c + l
+// 20 tensor boxes of 200 rows x 16 bytes in a staging buffer, S[2 x + c].  Thread 32 w + 16 c + l
 // works on pencil c at t = 16 w + l (< 200): each half-warp holds 16 consecutive t of one pencil.
+// Two staging buffers alternate between tiles.  Stage 1 reads the tile's buffer into registers and
+// writes exchange buffer A; stage 2 writes its outputs (buffer B) into the staging buffer the tile
+// has just been read from, and stage 3 reads them there.  The next tile but one is issued into that
+// buffer once every thread is past stage 3, so each tile has a whole tile's transforms to land
+// (the strided rows of a tile are far apart in memory and slow to gather).
 // MID: the rows run along the map's middle dimension and tile (o, b) reads boxes at (4 b, 200 j,
 // f nouter + o); otherwise along the outer dimension, boxes at (4 b, o, f nx + 200 j).
 // EPI false (MID): the z-fastest y pass (o = x); the folded segments are stored in place.
@@ -313,99 +318,112 @@ __global__ void __launch_bounds__(kT, 2) ypass4000(AxisArgs<float> a, const __gr
 // four neighbouring k_z that share each 32-byte sector of I write it together.
 // ---------------------------------------------------------------------------------------
 constexpr int kXT = 416;
-constexpr int kTile = 2 * kN;                 // staging: two pencils, interleaved
-constexpr int kPen = kSA + kSB + 8;           // one pencil's exchange buffers, the second 8 banks over
+constexpr int kTile = 2 * kN;                 // two pencils, interleaved
+constexpr int kBOff = kSB + 8;                // pencil 1's stage-2 outputs in a staging buffer, 8 banks over
+constexpr int kStage = 2 * kSB + 16;          // one staging buffer: a tile, later both pencils' B (128-byte multiple)
+constexpr int kAOff = kSA + 8;                // pencil 1's stage-1 outputs, 8 banks over
+static_assert(kStage >= kTile && kStage >= kBOff + kSB && (kStage * 8) % 128 == 0, "staging buffer layout");
 
 template <bool EPI, bool YZ, bool MID>
 __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CUtensorMap map, AxisArgs<float> a,
-                                                      const __grid_constant__ Pass4k p, int nouter, long long ntiles) {
+                                                      const __grid_constant__ Pass4k p, int nouter, int ntiles) {
     extern __shared__ __align__(128) unsigned char sm_raw[];
-    float2* S = reinterpret_cast<float2*>(sm_raw);
+    float2* S0 = reinterpret_cast<float2*>(sm_raw);  // staging buffers S0, S1
     const int tid = threadIdx.x;
     const int c = (tid >> 4) & 1;
     const int t = (tid >> 5) * 16 + (tid & 15);
     const bool act = t < kT;
     const int tt = act ? t : 0;
-    float2* A = S + kTile + c * kPen;
-    float2* B = A + kSA;
-    const Twiddles tw{S + kTile + 2 * kPen, S + kTile + 2 * kPen + kT2};
-    float2* Vs = S + kTile + 2 * kPen + kTW;
-    __shared__ __align__(8) uint64_t bar;
+    float2* A = S0 + 2 * kStage + c * kAOff;
+    const Twiddles tw{S0 + 2 * kStage + 2 * kAOff, S0 + 2 * kStage + 2 * kAOff + kT2};
+    float2* Vs = S0 + 2 * kStage + 2 * kAOff + kTW;
+    __shared__ __align__(8) uint64_t bar[2];
     if (smem_u32(sm_raw) % 128 != 0) {  // TMA destinations must be 128-byte aligned: refuse, do not load
         if (tid == 0) atomicExch(a.status, QPD_DEVERR_ALIGN);
         return;
     }
-    long long q = blockIdx.x;
+    int q = blockIdx.x;
     if (q >= ntiles) return;
     tw.fill(static_cast<const float2*>(a.ap.tw), tid, kXT);
     fill_v(Vs, p, tid, kXT);
-    const Lanes L(A, B, tt);
+    // stage-2/3 lanes of each staging buffer (B = that buffer + c kBOff)
+    const Lanes L0(A, S0 + c * kBOff, tt), L1(A, S0 + kStage + c * kBOff, tt);
     const int npairs = a.nz / 2;
     const int nfx = (int)a.nx;
     constexpr int GB = 40, GO = 4;  // YZ tile groups: k_y pairs x k_z
     const bool grouped = npairs % GB == 0 && nouter % GO == 0;
-    auto tile_of = [&](long long qq, int* o, int* b) {
+    auto tile_of = [&](int qq, int* o, int* b) {
         if (EPI && YZ) {
             if (grouped) {
-                const int in = (int)(qq % (GB * GO));
-                const long long g = qq / (GB * GO);
+                const int in = qq % (GB * GO);
+                const int g = qq / (GB * GO);
                 const int nog = nouter / GO;
-                *b = (int)(g / nog) * GB + in % GB;
-                *o = (int)(g % nog) * GO + in / GB;
+                *b = (g / nog) * GB + in % GB;
+                *o = (g % nog) * GO + in / GB;
             } else {
-                *o = (int)(qq % nouter);
-                *b = (int)(qq / nouter);
+                *o = qq % nouter;
+                *b = qq / nouter;
             }
         } else {
-            *o = (int)(qq / npairs);
-            *b = (int)(qq % npairs);
+            *o = qq / npairs;
+            *b = qq % npairs;
         }
     };
-    auto issue = [&](long long qq, int fl) {
+    auto issue = [&](int qq, int fl, int sb) {
         int o, b;
         tile_of(qq, &o, &b);
         const int f = p.field[fl];
-        mbar_expect_tx(&bar, kTile * sizeof(float2));
+        float2* dst = S0 + sb * kStage;
+        mbar_expect_tx(&bar[sb], kTile * sizeof(float2));
 #pragma unroll
         for (int j = 0; j < 20; j++) {
-            if (MID) tma_load_3d(S + 400 * j, &map, &bar, 4 * b, 200 * j, f * nouter + o);
-            else tma_load_3d(S + 400 * j, &map, &bar, 4 * b, o, f * nfx + 200 * j);
+            if (MID) tma_load_3d(dst + 400 * j, &map, &bar[sb], 4 * b, 200 * j, f * nouter + o);
+            else tma_load_3d(dst + 400 * j, &map, &bar[sb], 4 * b, o, f * nfx + 200 * j);
         }
     };
+    // the k-th step of this CTA: tile q0 + (k / n) gridDim.x, input k mod n
+    auto step_of = [&](int k, int* qq, int* fl) {
+        *qq = q + (k / p.n) * (int)gridDim.x;
+        *fl = k % p.n;
+    };
     if (tid == 0) {
-        mbar_init(&bar, 1);
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
         fence_barrier_init();
-        issue(q, 0);
+        for (int k = 0; k < 2; k++) {
+            int qq, fl;
+            step_of(k, &qq, &fl);
+            if (qq < ntiles) issue(qq, fl, k);
+        }
     }
     __syncthreads();
-    uint32_t phase = 0;
     int fl = 0;
     float2 acc[20];
 #pragma unroll
     for (int r = 0; r < 20; r++) acc[r] = make_float2(0.f, 0.f);
-    for (;;) {
+    for (int k = 0;; k++) {
+        const int sb = k & 1;
         const float2 u = p.u[fl][tt];
-        long long nq = q;
-        int nfl = fl + 1;
-        if (nfl == p.n) {
-            nfl = 0;
-            nq += gridDim.x;
-        }
-        const bool more = nq < ntiles;
-        const bool ok = mbar_wait(&bar, phase, a.status);
+        const bool ok = mbar_wait(&bar[sb], (k >> 1) & 1, a.status);
         if (!__syncthreads_and(ok)) return;  // a copy never landed; the status word records it
-        phase ^= 1;
+        if (tid == 0 && k >= 1) {
+            // every thread is past step k - 1, whose buffer is free: fetch step k + 1 into it
+            int qq, f2;
+            step_of(k + 1, &qq, &f2);
+            if (qq < ntiles) {
+                fence_proxy_async();
+                issue(qq, f2, sb ^ 1);
+            }
+        }
+        const float2* S = S0 + sb * kStage;
+        const Lanes& L = sb ? L1 : L0;
         float2 v[20];
         if (act) {
 #pragma unroll
             for (int r = 0; r < 20; r++) v[r] = S[2 * (tt + 200 * r) + c];
             stage1(v, L);
         }
-        __syncthreads();  // A written, S consumed
-        if (tid == 0 && more) {
-            fence_proxy_async();
-            issue(nq, nfl);
-        }
+        __syncthreads();  // A written, the staging buffer consumed: stage 2 writes over it
         if (act) stage2(v, L, tw);
         __syncthreads();
         if (act) {
@@ -413,7 +431,7 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
             fold20(acc, v, u, Vs + 20 * fl, (p.ik >> fl) & 1, p.kscale, tt);
             if ((p.last >> fl) & 1) {
                 int o, b;
-                tile_of(q, &o, &b);
+                tile_of(q + (k / p.n) * (int)gridDim.x, &o, &b);
                 const int i = 2 * b + c;
                 if constexpr (EPI) {
                     const int ky = YZ ? i : o, kz = YZ ? o : i;
@@ -421,13 +439,17 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
                     const long long sy = shift_at(ky, NY);
                     const long long sz = shift_at(kz, NZ);
                     const double syz = a.S[1][ky] * a.S[2][kz];
+                    // y-fastest fields: the pencil's row of the staged (k_z, k_y, k_x) intensity, written whole
+                    // (the fftshifted I has k_z fastest, so writing it here would scatter single values)
+                    double* srow = YZ && a.Istage ? a.Istage + ((long long)kz * NY + ky) * nfx : nullptr;
 #pragma unroll
                     for (int r = 0; r < 20; r++) {
                         const int kx = tt + 200 * r;
                         const double Sx = a.S[0][kx] * syz;
                         const double re = (double)acc[r].x, im = (double)acc[r].y;
                         const double val = floor_1e50(Sx * Sx * (re * re + im * im) * a.scale2);
-                        a.I[((long long)shift_at(kx, nfx) * NY + sy) * NZ + sz] = val;
+                        if (srow) srow[kx] = val;
+                        else a.I[((long long)shift_at(kx, nfx) * NY + sy) * NZ + sz] = val;
                     }
                 } else {
                     float2* dst = a.out + (long long)p.out[fl] * a.fstride + (long long)o * a.ostride + i +
@@ -440,9 +462,38 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
                 for (int r = 0; r < 20; r++) acc[r] = make_float2(0.f, 0.f);
             }
         }
-        if (!more) break;
-        q = nq;
-        fl = nfl;
+        int qn, fn;
+        step_of(k + 1, &qn, &fn);
+        if (qn >= ntiles) break;
+        fl = fn;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Staged intensity -> I: I[shift(k_x)][shift(k_y)][shift(k_z)] = T[k_z][k_y][k_x] (shift(k) = (k + n / 2) mod n).
+// A tile is one k_y and 32 neighbouring k_x over all k_z: 8 warps read its k_z rows of 32 values (256 bytes
+// each), then write its 32 I rows of nz values (contiguous, k_z fastest).  CTAs are persistent.
+// ---------------------------------------------------------------------------------------
+constexpr int kUT = 256;
+
+__global__ void __launch_bounds__(kUT) unstage_intensity(const double* __restrict__ T, double* __restrict__ I, int nx,
+                                                         int ny, int nz, int ntiles) {
+    extern __shared__ __align__(16) double tile[];  // [k_z][33]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nxb = (nx + 31) / 32;
+    for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
+        const int ky = q / nxb;
+        const int x0 = (q - ky * nxb) * 32;
+        const int kx = x0 + lane;
+        for (int kz = warp; kz < nz; kz += kUT / 32)
+            if (kx < nx) tile[kz * 33 + lane] = T[((long long)kz * ny + ky) * nx + kx];
+        __syncthreads();
+        const long long sy = shift_at(ky, ny);
+        for (int j = warp; j < 32 && x0 + j < nx; j += kUT / 32) {
+            double* row = I + ((long long)shift_at(x0 + j, nx) * ny + sy) * nz;
+            for (int kz = lane; kz < nz; kz += 32) row[shift_at(kz, nz)] = tile[kz * 33 + j];
+        }
+        __syncthreads();
     }
 }
 
@@ -461,16 +512,29 @@ cudaError_t launch_strided(const CUtensorMap& map, const AxisArgs<float>& a, con
                            cudaStream_t st) {
     if (a.N != kN || a.nx < 1 || a.nz % 2 != 0 || nouter < 1 || p.n < 1 || p.n > kPass4kMax)
         return cudaErrorInvalidValue;
-    const size_t smem = sizeof(float2) * (kTile + 2 * kPen + kTW + 20 * p.n);
+    const size_t smem = sizeof(float2) * (2 * kStage + 2 * kAOff + kTW + 20 * p.n);
     cudaError_t e = cudaFuncSetAttribute(strided4000<EPI, YZ, MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const long long ntiles = (long long)nouter * (a.nz / 2);
+    if (ntiles * p.n + 2LL * sm_count() * p.n >= (1LL << 31)) return cudaErrorInvalidValue;  // steps index in 32 bits
     const long long grid = std::min<long long>(ntiles, sm_count());
-    strided4000<EPI, YZ, MID><<<(unsigned)grid, kXT, smem, st>>>(map, a, p, nouter, ntiles);
+    strided4000<EPI, YZ, MID><<<(unsigned)grid, kXT, smem, st>>>(map, a, p, nouter, (int)ntiles);
     return cudaGetLastError();
 }
 
 }  // namespace
+
+cudaError_t launch_unstage_intensity(const double* T, double* I, long long nx, long long ny, long long nz,
+                                     cudaStream_t st) {
+    const long long ntiles = ny * ((nx + 31) / 32);
+    if (nx < 1 || ny < 1 || nz < 1 || nz > 4096 || ntiles >= (1LL << 31)) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(double) * 33 * nz;
+    cudaError_t e = cudaFuncSetAttribute(unstage_intensity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long long grid = std::min<long long>(ntiles, 4LL * sm_count());
+    unstage_intensity<<<(unsigned)grid, kUT, smem, st>>>(T, I, (int)nx, (int)ny, (int)nz, (int)ntiles);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_ypass4000(const AxisArgs<float>& a, const Pass4k& p, long long npencils, cudaStream_t st) {
     if (p.n < 1 || p.n > kPass4kMax || npencils < 1) return cudaErrorInvalidValue;
