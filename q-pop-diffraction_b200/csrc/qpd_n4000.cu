@@ -298,46 +298,64 @@ __global__ void __launch_bounds__(kT, 2) ypass4000(AxisArgs<float> a, const __gr
     }
 }
 
+// Named barrier `id` over the n threads (a multiple of 32) of one pencil group.
+__device__ __forceinline__ void group_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+
+// The same barrier, returning whether p holds in every thread of the group.
+__device__ __forceinline__ bool group_and(bool p, int id, int n) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred pi, po;\n\t"
+        "setp.ne.u32 pi, %1, 0;\n\t"
+        "bar.red.and.pred po, %2, %3, pi;\n\t"
+        "selp.u32 %0, 1, 0, po;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(id), "r"(n)
+        : "memory");
+    return r != 0;
+}
+
 // ---------------------------------------------------------------------------------------
 // Strided pass: a tile is the two pencils of inner values 2 b and 2 b + 1 at one outer index o (the
 // value at transform index x of pencil (o, i) is element (o, i, x) of the map's view); it arrives as
-// 20 tensor boxes of 200 rows x 16 bytes in a staging buffer, S[2 x + c].  Thread 32 w + 16 c + l
-// works on pencil c at t = 16 w + l (< 200): each half-warp holds 16 consecutive t of one pencil.
-// Two staging buffers alternate between tiles.  Stage 1 reads the tile's buffer into registers and
-// writes exchange buffer A; stage 2 writes its outputs (buffer B) into the staging buffer the tile
-// has just been read from, and stage 3 reads them there.  The next tile but one is issued into that
-// buffer once every thread is past stage 3, so each tile has a whole tile's transforms to land
-// (the strided rows of a tile are far apart in memory and slow to gather).
+// 20 tensor boxes of 200 rows x 16 bytes in the staging buffer, S[2 x + c].  The CTA is two groups of
+// 7 warps, group c transforming pencil c (thread 32 w + l of the group at t = 32 w + l < 200), each with
+// its own exchange buffers and named barrier, so one pencil's barrier waits do not hold the other's
+// warps.  The groups share only the staging buffer: a group's leader counts its release in `released`
+// after the group's stage-1 reads, and the leader that completes the pair issues the next tile.
 // MID: the rows run along the map's middle dimension and tile (o, b) reads boxes at (4 b, 200 j,
 // f nouter + o); otherwise along the outer dimension, boxes at (4 b, o, f nx + 200 j).
 // EPI false (MID): the z-fastest y pass (o = x); the folded segments are stored in place.
 // EPI true: the x pass with the |S Amp|^2 + fftshift epilogue, YZ for y-fastest fields (o = k_z,
 // i = k_y; MID: (k_z, x, y) fields, whose x rows are ny values apart), else (x, y, z) fields (o = k_y,
 // i = k_z, i fastest).  YZ tiles go in groups of 40 k_y pairs x 4 k_z (k_y pair fastest) when the
-// extents allow: the tiles in flight then read 640 contiguous bytes of each x row per k_z, and the
-// four neighbouring k_z that share each 32-byte sector of I write it together.
+// extents allow, so the tiles in flight read 640 contiguous bytes of each x row per k_z.  With YZ and
+// AxisArgs::Istage set, each pencil's intensities go whole into the staged (k_z, k_y, k_x) rows and
+// unstage_intensity moves them to I afterwards: written here, the fftshifted I (k_z fastest) would
+// take every value in a sector of its own.
 // ---------------------------------------------------------------------------------------
-constexpr int kXT = 416;
-constexpr int kTile = 2 * kN;                 // two pencils, interleaved
-constexpr int kBOff = kSB + 8;                // pencil 1's stage-2 outputs in a staging buffer, 8 banks over
-constexpr int kStage = 2 * kSB + 16;          // one staging buffer: a tile, later both pencils' B (128-byte multiple)
-constexpr int kAOff = kSA + 8;                // pencil 1's stage-1 outputs, 8 banks over
-static_assert(kStage >= kTile && kStage >= kBOff + kSB && (kStage * 8) % 128 == 0, "staging buffer layout");
+constexpr int kGT = 7 * 32;                  // threads of one pencil group
+constexpr int kXT = 2 * kGT;                  // two groups
+constexpr int kTile = 2 * kN;                 // staging: two pencils, interleaved
+constexpr int kPen = kSA + kSB + 8;           // one pencil's exchange buffers, the second 8 banks over
 
 template <bool EPI, bool YZ, bool MID>
 __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CUtensorMap map, AxisArgs<float> a,
                                                       const __grid_constant__ Pass4k p, int nouter, int ntiles) {
     extern __shared__ __align__(128) unsigned char sm_raw[];
-    float2* S0 = reinterpret_cast<float2*>(sm_raw);  // staging buffers S0, S1
+    float2* S = reinterpret_cast<float2*>(sm_raw);
     const int tid = threadIdx.x;
-    const int c = (tid >> 4) & 1;
-    const int t = (tid >> 5) * 16 + (tid & 15);
+    const int c = tid / kGT;
+    const int t = tid - c * kGT;
+    const int gbar = 1 + c;  // the group's named barrier (0 is __syncthreads)
     const bool act = t < kT;
     const int tt = act ? t : 0;
-    float2* A = S0 + 2 * kStage + c * kAOff;
-    const Twiddles tw{S0 + 2 * kStage + 2 * kAOff, S0 + 2 * kStage + 2 * kAOff + kT2};
-    float2* Vs = S0 + 2 * kStage + 2 * kAOff + kTW;
-    __shared__ __align__(8) uint64_t bar[2];
+    float2* A = S + kTile + c * kPen;
+    float2* B = A + kSA;
+    const Twiddles tw{S + kTile + 2 * kPen, S + kTile + 2 * kPen + kT2};
+    float2* Vs = S + kTile + 2 * kPen + kTW;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ unsigned int released;  // +1 per group and tile once the group has read the staging buffer
     if (smem_u32(sm_raw) % 128 != 0) {  // TMA destinations must be 128-byte aligned: refuse, do not load
         if (tid == 0) atomicExch(a.status, QPD_DEVERR_ALIGN);
         return;
@@ -346,13 +364,12 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
     if (q >= ntiles) return;
     tw.fill(static_cast<const float2*>(a.ap.tw), tid, kXT);
     fill_v(Vs, p, tid, kXT);
-    // stage-2/3 lanes of each staging buffer (B = that buffer + c kBOff)
-    const Lanes L0(A, S0 + c * kBOff, tt), L1(A, S0 + kStage + c * kBOff, tt);
+    const Lanes L(A, B, tt);
     const int npairs = a.nz / 2;
     const int nfx = (int)a.nx;
     constexpr int GB = 40, GO = 4;  // YZ tile groups: k_y pairs x k_z
     const bool grouped = npairs % GB == 0 && nouter % GO == 0;
-    auto tile_of = [&](int qq, int* o, int* b) {
+    auto tile_of = [&](int qq, int* o, int* b) {  // 32-bit: ntiles < 2^31 (checked at launch)
         if (EPI && YZ) {
             if (grouped) {
                 const int in = qq % (GB * GO);
@@ -369,69 +386,66 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
             *b = qq % npairs;
         }
     };
-    auto issue = [&](int qq, int fl, int sb) {
+    auto issue = [&](int qq, int fl) {
         int o, b;
         tile_of(qq, &o, &b);
         const int f = p.field[fl];
-        float2* dst = S0 + sb * kStage;
-        mbar_expect_tx(&bar[sb], kTile * sizeof(float2));
+        mbar_expect_tx(&bar, kTile * sizeof(float2));
 #pragma unroll
         for (int j = 0; j < 20; j++) {
-            if (MID) tma_load_3d(dst + 400 * j, &map, &bar[sb], 4 * b, 200 * j, f * nouter + o);
-            else tma_load_3d(dst + 400 * j, &map, &bar[sb], 4 * b, o, f * nfx + 200 * j);
+            if (MID) tma_load_3d(S + 400 * j, &map, &bar, 4 * b, 200 * j, f * nouter + o);
+            else tma_load_3d(S + 400 * j, &map, &bar, 4 * b, o, f * nfx + 200 * j);
         }
-    };
-    // the k-th step of this CTA: tile q0 + (k / n) gridDim.x, input k mod n
-    auto step_of = [&](int k, int* qq, int* fl) {
-        *qq = q + (k / p.n) * (int)gridDim.x;
-        *fl = k % p.n;
     };
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        mbar_init(&bar, 1);
         fence_barrier_init();
-        for (int k = 0; k < 2; k++) {
-            int qq, fl;
-            step_of(k, &qq, &fl);
-            if (qq < ntiles) issue(qq, fl, k);
-        }
+        released = 0;
+        issue(q, 0);
     }
     __syncthreads();
+    uint32_t phase = 0;
     int fl = 0;
     float2 acc[20];
 #pragma unroll
     for (int r = 0; r < 20; r++) acc[r] = make_float2(0.f, 0.f);
-    for (int k = 0;; k++) {
-        const int sb = k & 1;
+    for (;;) {
         const float2 u = p.u[fl][tt];
-        const bool ok = mbar_wait(&bar[sb], (k >> 1) & 1, a.status);
-        if (!__syncthreads_and(ok)) return;  // a copy never landed; the status word records it
-        if (tid == 0 && k >= 1) {
-            // every thread is past step k - 1, whose buffer is free: fetch step k + 1 into it
-            int qq, f2;
-            step_of(k + 1, &qq, &f2);
-            if (qq < ntiles) {
-                fence_proxy_async();
-                issue(qq, f2, sb ^ 1);
-            }
+        int nq = q;
+        int nfl = fl + 1;
+        if (nfl == p.n) {
+            nfl = 0;
+            nq += gridDim.x;
         }
-        const float2* S = S0 + sb * kStage;
-        const Lanes& L = sb ? L1 : L0;
+        const bool more = nq < ntiles;
+        const bool ok = mbar_wait(&bar, phase, a.status);
+        if (!group_and(ok, gbar, kGT)) return;  // a copy never landed; the status word records it
+        phase ^= 1;
         float2 v[20];
         if (act) {
 #pragma unroll
             for (int r = 0; r < 20; r++) v[r] = S[2 * (tt + 200 * r) + c];
             stage1(v, L);
         }
-        __syncthreads();  // A written, the staging buffer consumed: stage 2 writes over it
+        group_sync(gbar, kGT);  // A written, this group's reads of S done
+        if (t == 0 && more) {
+            // the second group to release the staging buffer issues the next tile into it
+            __threadfence_block();
+            const unsigned int before = atomicAdd(&released, 1u);
+            __threadfence_block();
+            if (before & 1u) {
+                fence_proxy_async();
+                issue(nq, nfl);
+            }
+        }
         if (act) stage2(v, L, tw);
-        __syncthreads();
+        group_sync(gbar, kGT);
         if (act) {
             stage3(v, L, tw);
             fold20(acc, v, u, Vs + 20 * fl, (p.ik >> fl) & 1, p.kscale, tt);
             if ((p.last >> fl) & 1) {
                 int o, b;
-                tile_of(q + (k / p.n) * (int)gridDim.x, &o, &b);
+                tile_of(q, &o, &b);
                 const int i = 2 * b + c;
                 if constexpr (EPI) {
                     const int ky = YZ ? i : o, kz = YZ ? o : i;
@@ -439,8 +453,6 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
                     const long long sy = shift_at(ky, NY);
                     const long long sz = shift_at(kz, NZ);
                     const double syz = a.S[1][ky] * a.S[2][kz];
-                    // y-fastest fields: the pencil's row of the staged (k_z, k_y, k_x) intensity, written whole
-                    // (the fftshifted I has k_z fastest, so writing it here would scatter single values)
                     double* srow = YZ && a.Istage ? a.Istage + ((long long)kz * NY + ky) * nfx : nullptr;
 #pragma unroll
                     for (int r = 0; r < 20; r++) {
@@ -462,10 +474,9 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
                 for (int r = 0; r < 20; r++) acc[r] = make_float2(0.f, 0.f);
             }
         }
-        int qn, fn;
-        step_of(k + 1, &qn, &fn);
-        if (qn >= ntiles) break;
-        fl = fn;
+        if (!more) break;
+        q = nq;
+        fl = nfl;
     }
 }
 
@@ -512,11 +523,11 @@ cudaError_t launch_strided(const CUtensorMap& map, const AxisArgs<float>& a, con
                            cudaStream_t st) {
     if (a.N != kN || a.nx < 1 || a.nz % 2 != 0 || nouter < 1 || p.n < 1 || p.n > kPass4kMax)
         return cudaErrorInvalidValue;
-    const size_t smem = sizeof(float2) * (2 * kStage + 2 * kAOff + kTW + 20 * p.n);
+    const size_t smem = sizeof(float2) * (kTile + 2 * kPen + kTW + 20 * p.n);
     cudaError_t e = cudaFuncSetAttribute(strided4000<EPI, YZ, MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const long long ntiles = (long long)nouter * (a.nz / 2);
-    if (ntiles * p.n + 2LL * sm_count() * p.n >= (1LL << 31)) return cudaErrorInvalidValue;  // steps index in 32 bits
+    if (ntiles + sm_count() >= (1LL << 31)) return cudaErrorInvalidValue;  // tiles index in 32 bits
     const long long grid = std::min<long long>(ntiles, sm_count());
     strided4000<EPI, YZ, MID><<<(unsigned)grid, kXT, smem, st>>>(map, a, p, nouter, (int)ntiles);
     return cudaGetLastError();
