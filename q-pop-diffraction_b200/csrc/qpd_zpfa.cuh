@@ -18,6 +18,9 @@
 // Shared memory is written and read once per value and atom (the Stockham z stage does it three
 // times).  The fold coefficients are permuted into the same (a, r) order once per CTA.  Item orders
 // and the pencil stride were chosen with a bank model so that the phase-B loads are conflict-free.
+// Two exchange buffers let phase A of the next atom run in the same barrier interval as phase B of
+// the current one (one CTA barrier per atom); the tile's inputs move to registers at its start, so a
+// single input buffer takes the next tile's bulk copies while the atoms run.
 #pragma once
 
 #include "qpd_fast.cuh"
@@ -69,8 +72,9 @@ template <typename T, int N1, int N2> struct ZPfaLayout {
     static constexpr int CELLS16 = (CELLS + 15) / 16 * 16;
     static constexpr size_t BUF = sizeof(C_t<T>) * 4 * PLANE;
     static constexpr size_t INB = (sizeof(T) * 7 * CELLS + CELLS16 + 15) / 16 * 16;
+    // two exchange buffers (one per atom in flight), one input buffer
     static size_t bytes(int nap, int nAtom) {
-        return BUF + 2 * INB + sizeof(AtomPhase<T>) * nap + sizeof(C_t<T>) * 2 * nAtom * NZ + 64;
+        return 2 * BUF + INB + sizeof(AtomPhase<T>) * nap + sizeof(C_t<T>) * 2 * nAtom * NZ + 64;
     }
 };
 
@@ -86,12 +90,13 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
     static_assert(IA <= NT && IB <= NT && NT % 32 == 0, "one phase-A and one phase-B item per thread");
     static_assert(SPLIT == 1 || (SPLIT == 2 && N1 == 8), "lane pairs split an 8-point DFT only");
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    C* buf = reinterpret_cast<C*>(smem_raw);
-    unsigned char* inb = smem_raw + L::BUF;
-    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(inb + 2 * L::INB);
+    C* const xb0 = reinterpret_cast<C*>(smem_raw);  // exchange buffers: atom at uses xb[at & 1]
+    C* const xb1 = xb0 + 4 * PLANE;
+    unsigned char* inb = smem_raw + 2 * L::BUF;
+    AtomPhase<T>* apc = reinterpret_cast<AtomPhase<T>*>(inb + L::INB);
     C* sce = reinterpret_cast<C*>(apc + a.in.nPhase * a.nAtom);
     C* scu = sce + a.nAtom * NZ;
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t bar;
     const int tid = threadIdx.x;
     const int nap = a.in.nPhase * a.nAtom;
     for (int i = tid; i < nap; i += NT) apc[i] = a.apc[i];
@@ -113,32 +118,26 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
     constexpr bool TILE_BULK = (CELLS * sizeof(T)) % 16 == 0 && CELLS % 16 == 0;
     const bool bulk_mode = aligned && TILE_BULK;
     auto bulk_ok = [&](long long t) { return bulk_mode && ncell_of(t) == CELLS; };
-    auto issue = [&](long long t, int b) {
+    T* const sin_ = reinterpret_cast<T*>(inb);
+    T* const swt = sin_ + 6 * CELLS;
+    signed char* const sph = reinterpret_cast<signed char*>(swt + CELLS);
+    auto issue = [&](long long t) {
         const long long g0 = t * M * NZ;
-        T* sin_ = reinterpret_cast<T*>(inb + b * L::INB);
-        T* swt = sin_ + 6 * CELLS;
-        signed char* sph = reinterpret_cast<signed char*>(swt + CELLS);
         const uint32_t pb = CELLS * sizeof(T);
-        mbar_expect_tx(&bar[b], 6 * pb + CELLS + (a.in.weight ? pb : 0));
+        mbar_expect_tx(&bar, 6 * pb + CELLS + (a.in.weight ? pb : 0));
         for (int k = 0; k < 3; k++) {
-            bulk_load(sin_ + k * CELLS, a.in.P + k * a.in.n + g0, pb, &bar[b]);
-            bulk_load(sin_ + (3 + k) * CELLS, a.in.U + k * a.in.n + g0, pb, &bar[b]);
+            bulk_load(sin_ + k * CELLS, a.in.P + k * a.in.n + g0, pb, &bar);
+            bulk_load(sin_ + (3 + k) * CELLS, a.in.U + k * a.in.n + g0, pb, &bar);
         }
-        bulk_load(sph, a.in.phase + g0, CELLS, &bar[b]);
-        if (a.in.weight) bulk_load(swt, a.in.weight + g0, pb, &bar[b]);
+        bulk_load(sph, a.in.phase + g0, CELLS, &bar);
+        if (a.in.weight) bulk_load(swt, a.in.weight + g0, pb, &bar);
     };
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        mbar_init(&bar, 1);
         fence_barrier_init();
     }
     __syncthreads();
-    if (tid == 0) {
-        for (int k = 0; k < 2; k++) {
-            const long long t = blockIdx.x + (long long)k * gridDim.x;
-            if (t < ntiles && bulk_ok(t)) issue(t, k);
-        }
-    }
+    if (tid == 0 && (long long)blockIdx.x < ntiles && bulk_ok(blockIdx.x)) issue(blockIdx.x);
 
     // this thread's items
     int am, ab, ah;
@@ -156,24 +155,64 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
         zc[j] = v >= NZ ? v - NZ : v;
     }
 
+    // phase A of atom at: sources of this thread's cells, stage-1 DFT, one store per value into dst
+    auto phase_a = [&](int at, C* dst, const CellIn<T> (&cl)[CPA], const int (&cph)[CPA], const T (&cwt)[CPA]) {
+        if (!warpA) return;
+        C src[4][CPA];
+#pragma unroll
+        for (int j = 0; j < CPA; j++) {
+            C E = cmake<C>(0, 0), X = E, Y = E, Z = E;
+            if (cph[j] >= 0 && cph[j] < a.in.nPhase) add_source<T>(cl[j], apc[cph[j] * a.nAtom + at], cwt[j], E, X, Y, Z);
+            src[0][j] = E;
+            src[1][j] = X;
+            src[2][j] = Y;
+            src[3][j] = Z;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            C* plane = dst + q * PLANE + am * PS;
+            if constexpr (SPLIT == 2) {
+                C v[4] = {src[q][0], src[q][1], src[q][2], src[q][3]};
+                dft4(v[0], v[1], v[2], v[3]);
+                if (ah) {  // odd half: exp(-2 pi i k / 8) O_k
+                    using R_t = decltype(C::x);
+                    const R_t r2 = R_t(0.70710678118654752440);
+                    const C o1 = v[1], o3 = v[3];
+                    v[1] = cmake<C>((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);
+                    v[2] = cmul_mi(v[2]);
+                    v[3] = cmake<C>((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);
+                }
+                C* row = plane + 4 * N2 * ah + ab;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    C p;
+                    p.x = __shfl_xor_sync(0xffffffffu, v[k].x, 1);
+                    p.y = __shfl_xor_sync(0xffffffffu, v[k].y, 1);
+                    // even lane: X_k = E_k + O'_k; odd lane: X_{k+4} = E_k - O'_k
+                    const C x = ah ? csub(p, v[k]) : cadd(v[k], p);
+                    if (actA) row[k * N2] = x;
+                }
+            } else {
+                C v[N1];
+#pragma unroll
+                for (int j = 0; j < N1; j++) v[j] = src[q][j];
+                Dft<N1, C>::run(v);
+#pragma unroll
+                for (int k = 0; k < N1; k++)
+                    if (actA) plane[k * N2 + ab] = v[k];
+            }
+        }
+    };
+
     for (int it = 0;; it++) {
         const long long t = blockIdx.x + (long long)it * gridDim.x;
         if (t >= ntiles) break;
-        const int b = it & 1;
         const int ncell = ncell_of(t);
         const long long g0 = t * M * NZ;
-        T* sin_ = reinterpret_cast<T*>(inb + b * L::INB);
-        T* swt = sin_ + 6 * CELLS;
-        signed char* sph = reinterpret_cast<signed char*>(swt + CELLS);
         if (bulk_ok(t)) {
-            const bool ok = mbar_wait(&bar[b], (it >> 1) & 1, a.status);
-            if (!__syncthreads_and(ok)) {
-                if (tid == 0) {
-                    const long long t2 = t + gridDim.x;
-                    if (t2 < ntiles && bulk_ok(t2)) mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, nullptr);
-                }
-                return;
-            }
+            // every tile but a partial last one is bulk-loaded, so this is the CTA's it-th use of bar
+            const bool ok = mbar_wait(&bar, it & 1, a.status);
+            if (!__syncthreads_and(ok)) return;  // the copy never landed (nothing else is in flight)
         } else {
             for (int e = tid; e < ncell; e += NT) {
                 for (int k = 0; k < 3; k++) {
@@ -208,13 +247,14 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
             }
             cl[j].tu = a.tq[0] * (double)cl[j].u[0] + a.tq[1] * (double)cl[j].u[1] + a.tq[2] * (double)cl[j].u[2];
         }
+        phase_a(0, xb0, cl, cph, cwt);
         __syncthreads();
-        // the input buffer is free: fetch the tile two steps ahead into it
+        // the input buffer is free: fetch the next tile into it while this one's atoms run
         if (tid == 0) {
-            const long long t2 = t + 2LL * gridDim.x;
+            const long long t2 = t + gridDim.x;
             if (t2 < ntiles && bulk_ok(t2)) {
                 fence_proxy_async();
-                issue(t2, b);
+                issue(t2);
             }
         }
 
@@ -223,57 +263,12 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
         for (int r = 0; r < N2; r++) acc[r] = cmake<C>(0, 0);
 
         for (int at = 0; at < a.nAtom; at++) {
-            // ---- phase A: sources of this thread's cells, stage-1 DFT, one store per value
-            if (warpA) {
-                C src[4][CPA];
-#pragma unroll
-                for (int j = 0; j < CPA; j++) {
-                    C E = cmake<C>(0, 0), X = E, Y = E, Z = E;
-                    if (cph[j] >= 0 && cph[j] < a.in.nPhase) add_source<T>(cl[j], apc[cph[j] * a.nAtom + at], cwt[j], E, X, Y, Z);
-                    src[0][j] = E;
-                    src[1][j] = X;
-                    src[2][j] = Y;
-                    src[3][j] = Z;
-                }
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    C* plane = buf + q * PLANE + am * PS;
-                    if constexpr (SPLIT == 2) {
-                        C v[4] = {src[q][0], src[q][1], src[q][2], src[q][3]};
-                        dft4(v[0], v[1], v[2], v[3]);
-                        if (ah) {  // odd half: exp(-2 pi i k / 8) O_k
-                            using R_t = decltype(C::x);
-                            const R_t r2 = R_t(0.70710678118654752440);
-                            const C o1 = v[1], o3 = v[3];
-                            v[1] = cmake<C>((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);
-                            v[2] = cmul_mi(v[2]);
-                            v[3] = cmake<C>((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);
-                        }
-                        C* row = plane + 4 * N2 * ah + ab;
-#pragma unroll
-                        for (int k = 0; k < 4; k++) {
-                            C p;
-                            p.x = __shfl_xor_sync(0xffffffffu, v[k].x, 1);
-                            p.y = __shfl_xor_sync(0xffffffffu, v[k].y, 1);
-                            // even lane: X_k = E_k + O'_k; odd lane: X_{k+4} = E_k - O'_k
-                            const C x = ah ? csub(p, v[k]) : cadd(v[k], p);
-                            if (actA) row[k * N2] = x;
-                        }
-                    } else {
-                        C v[N1];
-#pragma unroll
-                        for (int j = 0; j < N1; j++) v[j] = src[q][j];
-                        Dft<N1, C>::run(v);
-#pragma unroll
-                        for (int k = 0; k < N1; k++)
-                            if (actA) plane[k * N2 + ab] = v[k];
-                    }
-                }
-            }
-            __syncthreads();
+            C* const cur = (at & 1) ? xb1 : xb0;
+            // phase A of the next atom into the other buffer, then phase B of this one: one barrier per atom
+            if (at + 1 < a.nAtom) phase_a(at + 1, (at & 1) ? xb0 : xb1, cl, cph, cwt);
             // ---- phase B: stage-2 DFT of one component, folded into the accumulators
             if (actB) {
-                const C* row = buf + bc * PLANE + bm * PS + ba * N2;
+                const C* row = cur + bc * PLANE + bm * PS + ba * N2;
                 C v[N2];
 #pragma unroll
                 for (int r = 0; r < N2; r++) v[r] = row[r];
@@ -285,9 +280,11 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
             __syncthreads();
             const int g = a.grp[at];
             if (at == a.nAtom - 1 || a.grp[at + 1] != g) {
-                // the group's fields: accumulators in natural k_z order, then coalesced rows out
+                // the group's fields: accumulators in natural k_z order through this atom's buffer (its
+                // phase-B reads are done), then coalesced rows out
+                C* const ob = cur;
                 if (actB) {
-                    C* row = buf + bc * PLANE + bm * PS + ba * N2;
+                    C* row = ob + bc * PLANE + bm * PS + ba * N2;
 #pragma unroll
                     for (int r = 0; r < N2; r++) {
                         row[r] = acc[r];
@@ -305,9 +302,9 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
                         const int m = e - kz * mcols;
                         const long long d = kz * a.ncols + m;
                         const int s = m * PS + (kz % N1) * N2 + kz % N2;
-                        o[d] = cadd(buf[s], buf[3 * PLANE + s]);
-                        o[a.fstride + d] = buf[PLANE + s];
-                        o[2 * a.fstride + d] = buf[2 * PLANE + s];
+                        o[d] = cadd(ob[s], ob[3 * PLANE + s]);
+                        o[a.fstride + d] = ob[PLANE + s];
+                        o[2 * a.fstride + d] = ob[2 * PLANE + s];
                     }
                 } else if (a.yfast) {
                     // (x, k_z, y) layout: column c = x ny + y goes to (x nz + k_z) ny + y; neighbouring threads
@@ -325,9 +322,9 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
                         }
                         const long long d = (x * NZ + kz) * a.ny + y;
                         const int s = m * PS + (kz % N1) * N2 + kz % N2;
-                        o[d] = cadd(buf[s], buf[3 * PLANE + s]);
-                        o[a.fstride + d] = buf[PLANE + s];
-                        o[2 * a.fstride + d] = buf[2 * PLANE + s];
+                        o[d] = cadd(ob[s], ob[3 * PLANE + s]);
+                        o[a.fstride + d] = ob[PLANE + s];
+                        o[2 * a.fstride + d] = ob[2 * PLANE + s];
                     }
                 } else {
                     C* o = a.out + 3LL * g * a.fstride + g0;
@@ -335,12 +332,12 @@ __global__ void __launch_bounds__(ZPfa<N1, N2>::NT, 2) zstage_pfa(ZArgs<T> a) {
                         const int m = e / NZ;
                         const int kz = e - m * NZ;
                         const int s = m * PS + (kz % N1) * N2 + kz % N2;
-                        o[e] = cadd(buf[s], buf[3 * PLANE + s]);
-                        o[a.fstride + e] = buf[PLANE + s];
-                        o[2 * a.fstride + e] = buf[2 * PLANE + s];
+                        o[e] = cadd(ob[s], ob[3 * PLANE + s]);
+                        o[a.fstride + e] = ob[PLANE + s];
+                        o[2 * a.fstride + e] = ob[2 * PLANE + s];
                     }
                 }
-                __syncthreads();
+                __syncthreads();  // the buffer is phase A's again two atoms on
             }
         }
     }
