@@ -493,7 +493,8 @@ SERVING_HKLS = ((0, 0, 2), (1, 0, 3), (1, 1, 3), (2, 0, 0))
 
 # Engine options of the serving leg: stream priorities by grid size and at most two volumes in flight per
 # grid (measured on one B200: capacity 306 against 219 volumes/s with unlimited slots and no priorities,
-# p50 at 80% load 3.8 against 9.9 ms)
+# p50 at 80% load 3.8 against 9.9 ms); with priorities the engine also caps the tiles per CTA of the
+# persistent z stages (Engine cta_tiles), so a small volume does not wait out a large one's z stage
 SERVING_POLICY = {"priorities": True, "max_slots": 2}
 
 
@@ -533,7 +534,7 @@ def serving_leg(args, torch, device, policy=None):
                "capacity_volumes_per_s": cap["volumes_per_s"], "offered_rate_per_s": load["offered_rate_per_s"],
                "p50_ms": load["p50_ms"], "p99_ms": load["p99_ms"], "volumes_per_s": load["volumes_per_s"],
                "requests": load["requests"], "loads": loads,
-               "slots": eng.peak_slots, "policy": dict(policy), "hbm_budget_gb": budget / 1e9,
+               "slots": eng.peak_slots, "policy": dict(policy, cta_tiles=eng.cta_tiles), "hbm_budget_gb": budget / 1e9,
                "resident_snapshots_gb": store.nbytes / 1e9,
                "latency": "arrival to completion on the device, open-loop Poisson arrivals; p50/p99 at 80% of capacity, "
                           "loads: at 50, 80 and 95%, overall and per grid"}

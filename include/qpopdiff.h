@@ -196,6 +196,13 @@ QPD_API uint64_t qpd_launch_count(const qpd_ctx* ctx);
 QPD_API int qpd_enable_timing(qpd_ctx* ctx, int32_t on);
 QPD_API int qpd_stage_times(qpd_ctx* ctx, double* ms, uint64_t* counts, int32_t cap);
 
+/* Tiles per CTA of the persistent z stages (0, the default: one wave of CTAs walks all tiles of a
+ * volume).  With k > 0 every CTA takes at most k tiles, so CTAs retire while the kernel runs and a
+ * kernel on a higher-priority stream gets SMs within about k tiles' time instead of after the whole
+ * z stage: the serving loop uses it so that small volumes are not held behind a large one.  Results
+ * do not depend on it.  No counterpart in the reference (its z transform is a cuFFT/HeFFTe call). */
+QPD_API int qpd_set_cta_tiles(qpd_ctx* ctx, int32_t tiles);
+
 /* Reciprocal-space-map projections of a device-resident intensity I (nx, ny, nz) float64, z
  * fastest: xy[x * ny + y] = sum_z I, xz[x * nz + z] = sum_y I, yz[y * nz + z] = sum_x I (a NULL
  * output is skipped).  Deterministic: fixed summation order, no atomics.  With the tensor-product

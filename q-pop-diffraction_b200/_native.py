@@ -31,7 +31,7 @@ SCHEDULES = {"fused": QPD_SCHED_FUSED, "plain": QPD_SCHED_PLAIN}
 
 # Every symbol include/qpopdiff.h declares.
 EXPORTS = ("qpd_create", "qpd_destroy", "qpd_last_error", "qpd_plan", "qpd_set_crystal", "qpd_run_host",
-           "qpd_pack_device", "qpd_pack_fields", "qpd_run_device", "qpd_adjoint_device", "qpd_device_status", "qpd_probe_wait_timeout", "qpd_workspace_bytes", "qpd_launch_count", "qpd_enable_timing",
+           "qpd_pack_device", "qpd_pack_fields", "qpd_run_device", "qpd_adjoint_device", "qpd_device_status", "qpd_probe_wait_timeout", "qpd_workspace_bytes", "qpd_launch_count", "qpd_set_cta_tiles", "qpd_enable_timing",
            "qpd_stage_times", "qpd_run_device_noalloc", "qpd_rsm_project", "qpd_axis_radices")
 
 # Kernel kinds of qpd_stage_times (QPD_K_*), in index order.
@@ -104,6 +104,7 @@ def load(path=None):
         "qpd_probe_wait_timeout": (c_int, [c_void_p, c_int64]),
         "qpd_workspace_bytes": (c_uint64, [c_void_p]),
         "qpd_launch_count": (c_uint64, [c_void_p]),
+        "qpd_set_cta_tiles": (c_int, [c_void_p, c_int32]),
         "qpd_enable_timing": (c_int, [c_void_p, c_int32]),
         "qpd_stage_times": (c_int, [c_void_p, POINTER(c_double), POINTER(c_uint64), c_int32]),
         "qpd_run_device_noalloc": (c_int, [POINTER(QpdGrid), POINTER(QpdCrystal), c_void_p, c_void_p, c_void_p,

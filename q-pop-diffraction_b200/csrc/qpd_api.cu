@@ -125,6 +125,9 @@ struct qpd_ctx {
     // QPOP_B200_N4K=0: the 4000-point passes on the shared-memory Stockham kernels (axis_tma, axis_bulk)
     // instead of the register-resident ones of qpd_n4000.cu
     int knob_n4k = 1;
+    // qpd_set_cta_tiles: at most this many tiles per CTA of the persistent z stages (0: one wave of CTAs
+    // walks every tile)
+    int cta_tiles = 0;
     // QPOP_B200_OOP=0: in-place stages for the 256- and 512-point TMA passes (out-of-place measured
     // 1.080 against 1.104 ms for the y pass at 512x512x104)
     int knob_oop = 1;
@@ -856,6 +859,15 @@ template <typename T> struct Impl {
         return tstop(c, QPD_K_ZSTAGE, st, t0);
     }
 
+    // CTAs of a persistent z stage (each walks tiles gridDim.x apart): one wave of per_sm CTAs per SM, or
+    // with qpd_set_cta_tiles(k) enough CTAs that each takes at most k tiles, so that CTAs retire every k
+    // tiles and the block scheduler can start other streams' (higher-priority) kernels in between
+    static int64_t z_grid(const qpd_ctx* c, int64_t ntiles, int per_sm, int sms) {
+        const int64_t wave = (int64_t)std::max(per_sm, 1) * sms;
+        const int64_t grid = c->cta_tiles > 0 ? std::max(wave, (ntiles + c->cta_tiles - 1) / c->cta_tiles) : wave;
+        return std::max<int64_t>(1, std::min<int64_t>(ntiles, grid));
+    }
+
     template <int NZ, int M, int NT, class RAD, bool REGIN = false>
     static int smem_z_(qpd_ctx* c, ZArgs<T>& a, cudaStream_t st) {
         using L = ZLayout<T, NZ, M>;
@@ -869,7 +881,7 @@ template <typename T> struct Impl {
                                                                 smem));
         QPD_CU(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
         const int64_t ntiles = (a.ncols + M - 1) / M;
-        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sms));
+        const int64_t grid = z_grid(c, ntiles, per_sm, sms);
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
         zstage_pipe<T, NZ, M, NT, RAD, REGIN><<<(unsigned)grid, NT, smem, st>>>(a);
@@ -888,7 +900,7 @@ template <typename T> struct Impl {
         QPD_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zstage_pfa<T, N1, N2>, NT, smem));
         QPD_CU(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
         const int64_t ntiles = (a.ncols + L::M - 1) / L::M;
-        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sms));
+        const int64_t grid = z_grid(c, ntiles, per_sm, sms);
         cudaEvent_t t0;
         QPD_TRY(tstart(c, st, &t0));
         zstage_pfa<T, N1, N2><<<(unsigned)grid, NT, smem, st>>>(a);
@@ -1972,6 +1984,13 @@ int qpd_adjoint_device(qpd_ctx* c, const void* P, const void* U, const int8_t* p
     }
     Inputs<float> in = Impl<float>::inputs(c, P, U, phase, weight, wdense);
     return Impl<float>::adjoint(c, in, dI, static_cast<float*>(dP), static_cast<float*>(dU), st);
+}
+
+int qpd_set_cta_tiles(qpd_ctx* c, int32_t tiles) {
+    if (!c) return fail(c, QPD_ERR_ARG, "qpd_set_cta_tiles: ctx is NULL");
+    if (tiles < 0) return fail(c, QPD_ERR_ARG, "qpd_set_cta_tiles: tiles = %d must be >= 0", (int)tiles);
+    c->cta_tiles = tiles;
+    return QPD_OK;
 }
 
 int qpd_enable_timing(qpd_ctx* c, int32_t on) {

@@ -133,6 +133,11 @@ class Plan:
         """Run the bounded-wait failure path once (qpd_probe_wait_timeout); device_status() then raises."""
         self._check(self.lib.qpd_probe_wait_timeout(self._ctx, int(polls)))
 
+    def set_cta_tiles(self, tiles):
+        """At most `tiles` tiles per CTA of the persistent z stages (0: one wave of CTAs, the default), so
+        that kernels on higher-priority streams get SMs while this volume's z stage runs."""
+        self._check(self.lib.qpd_set_cta_tiles(self._ctx, int(tiles)))
+
     def enable_timing(self, on=True):
         """Record CUDA events around every kernel launch (see stage_times)."""
         self._check(self.lib.qpd_enable_timing(self._ctx, int(bool(on))))

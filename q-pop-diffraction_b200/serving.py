@@ -82,10 +82,11 @@ class Request:
 class Slot:
     """One in-flight volume's worth of resources for a grid shape."""
 
-    def __init__(self, shape, spacing, nPhase, device, crystal_of, priority=0):
+    def __init__(self, shape, spacing, nPhase, device, crystal_of, priority=0, cta_tiles=0):
         import torch
         self.shape, self.spacing = tuple(shape), tuple(spacing)
         self.plan = Plan(shape, spacing, nPhase, 3, precision="fp32", device=device)
+        self.plan.set_cta_tiles(cta_tiles)
         self.device = torch.device("cuda", device)
         self.stream = torch.cuda.Stream(self.device, priority=priority)
         self.out = torch.empty(self.shape, dtype=torch.float64, device=self.device)
@@ -126,11 +127,16 @@ class Engine:
     """Admission by HBM footprint, per-shape slots, continuous dispatch."""
 
     def __init__(self, store: SnapshotStore, hbm_budget_bytes, device=0, crystal_of=None, priorities=False,
-                 max_slots=None):
+                 max_slots=None, cta_tiles=None):
         """
         priorities: give the slots of smaller grids higher CUDA stream priorities, so that when SMs free
         up the block scheduler starts a small volume's kernels before a large one's.  max_slots: at most
         this many slots (volumes in flight) per grid shape; None: as many as the budget holds.
+        cta_tiles: tiles per CTA of the persistent z stages (Plan.set_cta_tiles); a persistent kernel
+        frees no SM until it ends, so without a limit a small volume waits out a large volume's whole
+        z stage whatever its priority.  None: 4 with priorities (a CTA of a 1024 x 1024 x 68 z stage then
+        lives about 60 microseconds), else 0 (one wave of CTAs).  Measured on one B200 over the 4-grid
+        mix at 80% load: p99 of the 128^3 requests 5.7 -> 0.96 ms (16 tiles: 1.3 ms), capacity unchanged.
         """
         from . import workloads
         self.store = store
@@ -138,6 +144,7 @@ class Engine:
         self.device = device
         self.priorities = priorities
         self.max_slots = max_slots
+        self.cta_tiles = (4 if priorities else 0) if cta_tiles is None else int(cta_tiles)
         self.crystal_of = crystal_of or (lambda params, hkl: crystal_from(params, workloads.serving_crystal(hkl)))
         self.slots = collections.defaultdict(list)   # shape -> [Slot]
         self.used = 0
@@ -158,7 +165,8 @@ class Engine:
         if self.max_slots is not None and len(self.slots[snap.shape]) >= self.max_slots:
             return None
         s = Slot(snap.shape, (params.dx, params.dy, params.dz), params.nPhase, self.device,
-                 lambda hkl, p=params: self.crystal_of(p, hkl), priority=self._priority(snap.shape))
+                 lambda hkl, p=params: self.crystal_of(p, hkl), priority=self._priority(snap.shape),
+                 cta_tiles=self.cta_tiles)
         self.used += s.footprint
         self.slots[snap.shape].append(s)
         self.peak_slots = max(self.peak_slots, sum(len(v) for v in self.slots.values()))

@@ -127,3 +127,26 @@ def test_cancel_queued_and_in_flight_requests(gpu):
         assert eng.release_idle() == 0
     finally:
         eng.close()
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 68), (96, 96, 104), (64, 64, 128)])
+def test_cta_tiles_do_not_change_results(gpu, shape):
+    """The serving loop caps the tiles per CTA of the persistent z stages (Plan.set_cta_tiles) so that
+    CTAs retire while a large volume runs; the volume's bits do not depend on the cap.  These grids
+    have more z-stage tiles than one wave of CTAs holds, so the caps really change the grid."""
+    torch = gpu
+    from qpop_diffraction_b200 import Plan, crystal_from, workloads
+    params, inputs = workloads.gpu_snapshot(workloads.TEXTURES[0], shape, seed=11, device="cuda")
+    crystal = crystal_from(params, workloads.serving_crystal((1, 0, 3)))
+    outs = []
+    for k in (0, 1, 3):
+        with Plan(shape, (params.dx, params.dy, params.dz), params.nPhase, 3, precision="fp32") as plan:
+            plan.set_crystal(crystal)
+            plan.set_cta_tiles(k)
+            out = torch.empty(shape, dtype=torch.float64, device="cuda")
+            plan.run_device(inputs, out)
+            torch.cuda.synchronize()
+            plan.device_status()
+            outs.append(out)
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
