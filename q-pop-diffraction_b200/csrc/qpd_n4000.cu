@@ -482,27 +482,30 @@ __global__ void __launch_bounds__(kXT, 1) strided4000(const __grid_constant__ CU
 
 // ---------------------------------------------------------------------------------------
 // Staged intensity -> I: I[shift(k_x)][shift(k_y)][shift(k_z)] = T[k_z][k_y][k_x] (shift(k) = (k + n / 2) mod n).
-// A tile is one k_y and 32 neighbouring k_x over all k_z: 8 warps read its k_z rows of 32 values (256 bytes
-// each), then write its 32 I rows of nz values (contiguous, k_z fastest).  CTAs are persistent.
+// A tile is one k_y and kUX neighbouring k_x over all k_z: 8 warps read its k_z rows of kUX values (512
+// bytes each), then write its kUX I rows of nz values (contiguous, k_z fastest).  CTAs are persistent.
 // ---------------------------------------------------------------------------------------
-constexpr int kUT = 256;
+constexpr int kUT = 256, kUX = 64, kUP = kUX + 1;  // threads, k_x per tile, padded shared row
 
 __global__ void __launch_bounds__(kUT) unstage_intensity(const double* __restrict__ T, double* __restrict__ I, int nx,
                                                          int ny, int nz, int ntiles) {
-    extern __shared__ __align__(16) double tile[];  // [k_z][33]
+    extern __shared__ __align__(16) double tile[];  // [k_z][kUP]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nxb = (nx + 31) / 32;
+    const int nxb = (nx + kUX - 1) / kUX;
     for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
         const int ky = q / nxb;
-        const int x0 = (q - ky * nxb) * 32;
-        const int kx = x0 + lane;
-        for (int kz = warp; kz < nz; kz += kUT / 32)
-            if (kx < nx) tile[kz * 33 + lane] = T[((long long)kz * ny + ky) * nx + kx];
+        const int x0 = (q - ky * nxb) * kUX;
+        for (int kz = warp; kz < nz; kz += kUT / 32) {
+            const double* row = T + ((long long)kz * ny + ky) * nx;
+#pragma unroll
+            for (int h = 0; h < kUX; h += 32)
+                if (x0 + h + lane < nx) tile[kz * kUP + h + lane] = row[x0 + h + lane];
+        }
         __syncthreads();
         const long long sy = shift_at(ky, ny);
-        for (int j = warp; j < 32 && x0 + j < nx; j += kUT / 32) {
+        for (int j = warp; j < kUX && x0 + j < nx; j += kUT / 32) {
             double* row = I + ((long long)shift_at(x0 + j, nx) * ny + sy) * nz;
-            for (int kz = lane; kz < nz; kz += 32) row[shift_at(kz, nz)] = tile[kz * 33 + j];
+            for (int kz = lane; kz < nz; kz += 32) row[shift_at(kz, nz)] = tile[kz * kUP + j];
         }
         __syncthreads();
     }
@@ -537,9 +540,9 @@ cudaError_t launch_strided(const CUtensorMap& map, const AxisArgs<float>& a, con
 
 cudaError_t launch_unstage_intensity(const double* T, double* I, long long nx, long long ny, long long nz,
                                      cudaStream_t st) {
-    const long long ntiles = ny * ((nx + 31) / 32);
-    if (nx < 1 || ny < 1 || nz < 1 || nz > 4096 || ntiles >= (1LL << 31)) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(double) * 33 * nz;
+    const long long ntiles = ny * ((nx + kUX - 1) / kUX);
+    if (nx < 1 || ny < 1 || nz < 1 || nz > 256 || ntiles >= (1LL << 31)) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(double) * kUP * nz;
     cudaError_t e = cudaFuncSetAttribute(unstage_intensity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const long long grid = std::min<long long>(ntiles, 4LL * sm_count());

@@ -51,7 +51,7 @@ cudaError_t launch_strided4000(const CUtensorMap& map, const AxisArgs<float>& a,
                                Strided4k kind, cudaStream_t st);
 
 // I[shift(k_x)][shift(k_y)][shift(k_z)] = T[k_z][k_y][k_x] for the intensity the y-fastest x pass staged in
-// AxisArgs::Istage (T and I distinct, nz <= 4096).
+// AxisArgs::Istage (T and I distinct, nz <= 256).
 cudaError_t launch_unstage_intensity(const double* T, double* I, long long nx, long long ny, long long nz,
                                      cudaStream_t st);
 
