@@ -408,6 +408,11 @@ def config3_leg(args, torch, dev, rank, world, shape=CONFIG3, steps=3, warmup=1,
            "ms_per_volume": ms, "value": replicas.throughput(n, ms * 1e-3, world) / 1e9, "unit": UNIT,
            "kernels": kernels, "peak_gbs": hbm, "peak_source": f"hbm_gbs of {hbm_src}",
            "device_memory_peak_gb": (torch.cuda.max_memory_allocated(dev) + plan.workspace_bytes) / 1e9}
+    # the model schedule's bytes (3 passes per atom and component, b_in = 25): A (25 + 144) per cell; the fused
+    # schedule moves about 290, so this fraction can exceed 1
+    model_cell = len(crystal.R) * (25 + 144)
+    res["model_roofline"] = {"bytes_per_cell": model_cell, "achieved_gbs": n * model_cell / (ms * 1e-3) / 1e9,
+                             "frac": n * model_cell / (ms * 1e-3) / 1e9 / hbm}
     if direct:
         vox, got = pick_voxels(torch, out)
         plan.close()
