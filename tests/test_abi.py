@@ -68,4 +68,5 @@ def test_null_arguments_are_rejected(lib):
     assert lib.qpd_create(0, 0, None) == _native.QPD_ERR_ARG
     assert lib.qpd_plan(None, None, 1, 3, 0, 0) == _native.QPD_ERR_ARG
     assert lib.qpd_run_device(None, None, None, None, None, None, None, None) == _native.QPD_ERR_ARG
+    assert lib.qpd_set_cta_tiles(None, 4) == _native.QPD_ERR_ARG
     assert lib.qpd_destroy(None) == _native.QPD_OK
